@@ -1,0 +1,360 @@
+"""Benchmark: Q4 64^3 matrix-free Laplacian apply (GDOF/s) and CG to relres
+1e-10, FP64 vs mixed precision, on one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one apply y = A x of the Q4 (p = 4), 5-point Gauss, 64^3-cell
+unit-cube problem with homogeneous Dirichlet boundary. The GDOF/s figure
+counts the 257^3 = 16,974,593 dofs of the mesh, boundary included. x is
+drawn from U[-1, 1] (seed 0) and is resident in HBM. Each timed step uses the
+next of 4 rotating x/y buffer pairs (1.09 GB in total, above the 126 MB L2),
+so a step never starts with its inputs in L2.
+
+With N > 1 (torchrun), every rank applies its own independent Q4 64^3
+problem: the apply of one problem has no exchange step in this
+configuration, so ranks are replicas (weak scaling). The timed region is
+bracketed by a barrier and a device synchronize, and the reported time is
+the maximum over ranks.
+
+``--impl reference`` times the reference's CPU path on this machine's host
+cores instead. Julia and Gridap are not available, so it runs the C
+restatement of the reference loops (oracle/sumfac_ref.c), using all host
+threads, on a bounded sample of the cells per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+P, DEG, NCELL = 4, 8, 64
+N_DOF_TOTAL = (NCELL * P + 1) ** 3  # 16,974,593
+METRIC = "Q4 64^3 Laplacian apply GDOF/s; CG time to relres 1e-10, mixed vs FP64, 1 B200"
+WORKLOAD = "Q4 64^3 affine hex, 5-pt Gauss, homogeneous Dirichlet, FP64 apply y=Ax"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cg", action="store_true", help="skip the CG solves")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+
+
+def build_problem(sf):
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (NCELL,) * 3)
+    V = sf.FESpace(model, P)
+    m = sf.SumFactorizationMap(3, (P,) * 3, (DEG,) * 3)
+    A = sf.LazyMatrix(m, V, V, sf.Measure(model, DEG))
+    return m, model, V, A
+
+
+def roofline_entry(achieved_gbs, peaks, traffic):
+    peak = peaks.get("hbm_gbs") if peaks else None
+    src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    return {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved_gbs / peak, 4), "traffic": traffic, "peak_source": src}
+
+
+def cpu_baseline_port(nsteps_full=3):
+    """The C restatement, 1 thread (the reference's mode), on full applies."""
+    from oracle import cref
+    from oracle import sumfac_oracle as O
+    m = O.make_map(3, P, DEG)
+    mesh = O.cartesian_mesh(3, NCELL, P, m)
+    cq = O.cell_quantities(m, mesh)
+    prob = cref.problem_from_oracle(m, mesh, cq)
+    x = np.random.default_rng(0).uniform(-1, 1, mesh.n_free)
+    y = np.empty(mesh.n_free)
+    prob.mul(x, y)  # warm-up (first touch)
+    t0 = time.perf_counter()
+    for _ in range(nsteps_full):
+        prob.mul(x, y)
+    t = (time.perf_counter() - t0) / nsteps_full
+    return {"value": round(N_DOF_TOTAL / t / 1e9, 6), "unit": "GDOF/s", "cores": 1, "kind": "port",
+            "sample": f"{nsteps_full} full Q4 64^3 applies after 1 warm-up, C restatement of the "
+                      f"reference loops (oracle/sumfac_ref.c), 1 thread; {t:.3f} s per apply"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__ as g
+
+    sf = g.load()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    m, model, V, A = build_problem(sf)
+    n = V.num_free_dofs
+    rng = np.random.default_rng(0 + rank)
+    x0 = torch.from_numpy(rng.uniform(-1, 1, n)).to(dev)
+    NBUF = 4
+    xs = [x0.clone() for _ in range(NBUF)]
+    ys = [torch.empty_like(x0) for _ in range(NBUF)]
+    stream = torch.cuda.current_stream()
+    for i in range(max(3, args.warmup)):
+        sf.mul(ys[i % NBUF], A, xs[i % NBUF])
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for i in range(args.steps):
+            sf.mul(ys[i % NBUF], A, xs[i % NBUF])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+    ms_step = ms / args.steps
+    value = world * N_DOF_TOTAL / (ms_step * 1e-3) / 1e9
+    kernel_path = "tiled-cartesian" if A.uses_tiled_kernel() else "general-element"
+
+    # end to end through the public host-buffer call (mul! on host vectors)
+    xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    yh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    xh[:] = x0.cpu().numpy()
+    for _ in range(3):
+        sf.mul(yh, A, xh)
+    ne2e = max(5, min(50, args.steps // 40))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ne2e):
+        sf.mul(yh, A, xh)
+    te2e = (time.perf_counter() - t0) / ne2e
+    if world > 1:
+        t = torch.tensor([te2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te2e = t.item()
+    e2e = {"value": round(world * N_DOF_TOTAL / te2e / 1e9, 4), "unit": "GDOF/s",
+           "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8,
+           "ms_per_step": round(te2e * 1e3, 4), "buffers": "pinned host, synchronous sf_mul_host"}
+
+    peaks = None
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    alg_bytes = N_DOF_TOTAL * 16
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GDOF/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: x ~ U[-1,1] seed 0 (rank r: seed r)",
+        "config": {"workload": WORKLOAD, "n_cells": NCELL ** 3, "order": P, "quad_points": 5,
+                   "n_dof_total": N_DOF_TOTAL, "n_free": n, "kernel": kernel_path,
+                   "l2": "4 rotating x/y pairs (1.09 GB) > 126 MB L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": e2e,
+        "gpu_launches": args.steps * A.kernels_per_apply(),
+        "roofline": roofline_entry(achieved, peaks, None),
+        "flops_reference_model": {"per_apply_gflop": 5.996544, "achieved_tflops":
+                                  round(5.996544 / (ms_step * 1e-3) / 1e3, 3)},
+    }
+    out["clocks"] = clk.summary()
+    out["roofline"]["algorithmic_bytes_per_launch"] = alg_bytes
+
+    if not args.no_cg:
+        out["cg"] = run_cg(sf, m, model, V, A, dev)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline_port()
+    if world > 1:
+        dist.barrier()
+    return out
+
+
+def run_cg(sf, m, model, V, A, dev):
+    import torch
+    b = torch.from_numpy(sf.assemble_rhs(m, V, lambda X: 3 * np.pi ** 2 * np.prod(np.sin(np.pi * X),
+                                                                               axis=-1))).to(dev)
+    X = V.free_dof_coordinates()
+    u_exact = torch.from_numpy(np.prod(np.sin(np.pi * X), axis=1)).to(dev)
+    res = {}
+    sols = {}
+    for mode in ("jacobi", "mixed"):
+        sf.cg(A, b, reltol=1e-10, mode=mode)  # warm-up: workspaces, diagonal
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x, info = sf.cg(A, b, reltol=1e-10, mode=mode)
+        e1.record()
+        torch.cuda.synchronize()
+        sols[mode] = x
+        res["f64" if mode == "jacobi" else "mixed"] = {
+            "ms": round(e0.elapsed_time(e1), 3), "iters": info["iters"], "outer": info["outer"],
+            "relres": info["relres"],
+            "err_vs_exact_max": (x - u_exact).abs().max().item(),
+        }
+    res["mixed"]["err_vs_f64_max_rel"] = ((sols["mixed"] - sols["jacobi"]).abs().max() /
+                                          sols["jacobi"].abs().max()).item()
+    res["speedup_mixed_vs_f64"] = round(res["f64"]["ms"] / res["mixed"]["ms"], 3)
+    res["preconditioner"] = "Jacobi (matrix-free diagonal)"
+    return res
+
+
+# ----------------------------------------------------------------------------
+# reference arm: the reference CPU path on the host cores
+# ----------------------------------------------------------------------------
+
+
+def run_reference(args):
+    from oracle import cref
+    from oracle import sumfac_oracle as O
+    m = O.make_map(3, P, DEG)
+    mesh = O.cartesian_mesh(3, NCELL, P, m)
+    cq = O.cell_quantities(m, mesh)
+    threads = cref.max_threads()
+    nc = mesh.cell_dof_ids.shape[0]
+    x = np.random.default_rng(0).uniform(-1, 1, mesh.n_free)
+    y = np.empty(mesh.n_free)
+    # calibrate: one full apply with all threads
+    full = cref.problem_from_oracle(m, mesh, cq)
+    full.mul(x, y, nthreads=threads)
+    t0 = time.perf_counter()
+    full.mul(x, y, nthreads=threads)
+    t_full = time.perf_counter() - t0
+    budget = 90.0  # seconds for warm-up + timed steps
+    frac = min(1.0, budget / max(1, args.steps + args.warmup) / max(t_full, 1e-9))
+    # sample: whole z-layers of cells, so the colouring stays valid
+    layers = max(1, int(round(frac * NCELL)))
+    cells = np.arange(layers * NCELL * NCELL)
+    wq, jq, djq = cq
+    sub_ids = mesh.cell_dof_ids[cells]
+    col, ncol = cref.cartesian_colors((NCELL, NCELL, layers))
+    prob = cref.Problem(m.A0, m.B0, m.dof_map, sub_ids, mesh.n_free, False, wq[cells], jq[cells],
+                        djq[cells], None, col, ncol)
+    for _ in range(args.warmup):
+        prob.mul(x, y, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        prob.mul(x, y, nthreads=threads)
+    t = (time.perf_counter() - t0) / args.steps
+    dofs = N_DOF_TOTAL * layers / NCELL
+    value = dofs / t / 1e9
+    sample = (f"{layers} of 64 z-layers of cells ({len(cells)} cells) per step; full apply "
+              f"{t_full:.3f} s with {threads} threads")
+    return {"metric": METRIC, "value": round(value, 6), "unit": "GDOF/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: x ~ U[-1,1] seed 0",
+            "config": {"workload": WORKLOAD, "n_cells": NCELL ** 3, "order": P, "quad_points": 5},
+            "impl": "reference",
+            "cpu_baseline": {"value": round(value, 6), "unit": "GDOF/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": "GDOF/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "Julia/Gridap absent: C restatement of src/SumFactorizationKernels.jl + "
+                    "src/LazyMatrices.jl mul! loops (oracle/sumfac_ref.c), colour-parallel"}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,177 @@
+/*
+ * sfb200.h -- C ABI of the B200 matrix-free sum-factorized Laplacian apply.
+ *
+ * This library replaces the CPU sum-factorization path of
+ * JordiManyer/NCIHackaton2023.jl at whole-operator granularity. The
+ * reference's per-cell Gridap Map protocol cannot cross into CUDA
+ * efficiently cell by cell, so the boundary sits at LinearAlgebra.mul!.
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (SF_OK == 0). No C++ exception crosses the ABI.
+ * When a call fails, sf_last_error(op) returns a message. A handle is not
+ * thread-safe; all device work is enqueued on the caller's stream.
+ *
+ * Array conventions follow the Julia reference: matrices are column-major,
+ * and indices in dof tables are 1-based. Free dofs are numbered 1..n_free;
+ * Dirichlet dofs carry negative ids and are read as zero and never written
+ * (src/GPUKernels.jl:23-27,86-88; test/Demo_StepByStep.jl:64-71).
+ */
+#ifndef SFB200_H
+#define SFB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sf_op sf_op;
+
+/* status codes */
+#define SF_OK 0
+#define SF_ERR_ARG 1          /* invalid argument (sizes, null pointers, unsupported order) */
+#define SF_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define SF_ERR_STATE 3        /* the handle is missing a required set-up step */
+#define SF_ERR_UNSUPPORTED 4  /* valid request that this build does not implement */
+#define SF_ERR_NOT_CONVERGED 5/* an iterative solve reached its iteration cap */
+#define SF_ERR_NONFINITE 6    /* NaN or Inf met in a solve */
+
+/* arithmetic types of x / y */
+#define SF_F64 0
+#define SF_F32 1
+
+/* CG modes for sf_cg */
+#define SF_CG_F64 0           /* FP64 Jacobi-preconditioned CG */
+#define SF_CG_MIXED 1         /* FP32 apply + FP32 inner Jacobi CG, FP64 outer refinement */
+#define SF_CG_F64_PLAIN 2     /* FP64 CG without a preconditioner (IterativeSolvers default) */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int sf_version(void);
+
+/* Text for a status code. */
+const char* sf_status_string(int status);
+
+/*
+ * Create an operator from the 1D data of a SumFactorizationMap.
+ * Replaces SumFactorizationMap(D, fe_orders, quad_orders)
+ * (src/SumFactorizationMaps.jl:47-65) plus to_gpu(m) (:25-32).
+ *   D       : 3 (this build); 2 is rejected with SF_ERR_UNSUPPORTED
+ *   SB, SQ  : 1D basis size p+1 (2..10) and quadrature size (1..10)
+ *   A0, B0  : SQ x SB column-major, A0[i + SQ*j] = phi_j(xi_i), B0 = phi_j'(xi_i)
+ *             (evalMats / B0 at src/SumFactorizationMaps.jl:53-54)
+ *   dof_map : SB^D x D column-major int32, 1-based: row k is the tensor index
+ *             (j1..jD) of local dof k (m.dof_map, src/SumFactorizationMaps.jl:40-45)
+ */
+int sf_create(sf_op** out, int D, int SB, int SQ, const double* A0, const double* B0,
+              const int32_t* dof_map);
+
+/* Free the handle and its device buffers. NULL is accepted. */
+int sf_destroy(sf_op* op);
+
+/* Last error message of this handle ("" if none). */
+const char* sf_last_error(const sf_op* op);
+
+/* get_dimensional_parameters(m) (src/SumFactorizationMaps.jl:15-17). */
+int sf_get_dimensional_parameters(const sf_op* op, int* D, int* SB, int* SQ);
+
+/*
+ * Cell-to-dof table as a Gridap Table (Utils.jl:12-15 to_gpu(::Table)).
+ *   ptrs : ncells+1 int32, 1-based offsets into data
+ *   data : local ids per cell in the local order of dof_map;
+ *          1..n_free free, negative Dirichlet
+ * This is get_cell_dof_ids(test) (src/LazyMatrices.jl:46).
+ */
+int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* data,
+                 int64_t n_free);
+
+/*
+ * Declare a Cartesian mesh: nx*ny*nz cells numbered with x fastest,
+ * Dirichlet on the whole boundary, and free dofs numbered lexicographically
+ * (x fastest) over the (nx*p-1) x (ny*p-1) x (nz*p-1) interior grid.
+ * node_order[j] (0-based) is the position 0..p of 1D basis function j along
+ * the segment; Gridap's order is {0, p, 1, 2, ..., p-1} (_get_terms,
+ * src/SumFactorizationMaps.jl:34-38). This selects the tiled Cartesian kernels.
+ */
+int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_order);
+
+/*
+ * Geometric factors at the quadrature points, exactly the triple
+ * (cell_wq, cell_jq, cell_djq) of LazyMatrix (src/LazyMatrices.jl:34-43):
+ *   wq  : SQ^D weights per cell (linear qp index, i1 fastest)
+ *   jq  : D x D per qp, column-major (jq[l + D*r] = jq[l,r]) = inv(grad cell map)
+ *   djq : |det| per qp
+ * fill = 1: the arrays hold ONE cell, shared by all cells (Gridap's Fill for
+ * Cartesian meshes); fill = 0: ncells consecutive blocks.
+ * The metric G = wq*djq*jq^T*jq (src/SumFactorizationKernels.jl:174-216) is
+ * formed once here and kept on the device (6 symmetric components per qp),
+ * or as a single constant when it is the same, up to the weights, everywhere.
+ */
+int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* jq,
+                           const double* djq);
+
+/* Diffusion coefficient kappa at every quadrature point (ncells x SQ^D) or
+ * NULL for kappa = 1. The operator becomes -div(kappa grad u). */
+int sf_set_coefficient(sf_op* op, const double* kappa);
+
+/*
+ * y = A x over the free dofs, device pointers, enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default). Replaces
+ * LinearAlgebra.mul!(y, A::LazyMatrix, x) (src/LazyMatrices.jl:52-61).
+ * dtype SF_F64 or SF_F32 (FP32 data and accumulation, FP64 metric).
+ */
+int sf_apply(sf_op* op, int dtype, const void* x, void* y, void* stream);
+
+/* nrhs right-hand sides: columns of length n_free at strides ldx / ldy (elements). */
+int sf_apply_multi(sf_op* op, int dtype, int nrhs, const void* x, int64_t ldx, void* y,
+                   int64_t ldy, void* stream);
+
+/* mul!(y, A, x) on HOST FP64 buffers (synchronous): copies x in, applies,
+ * copies y out. This is the drop-in for the reference's CPU mul!. */
+int sf_mul_host(sf_op* op, const double* x, double* y);
+
+/*
+ * The Map protocol itself: Arrays.evaluate!(cache, m, x, wq, jq, djq)
+ * (src/SumFactorizationMaps.jl:78-89) for a batch of cells, device pointers.
+ * x_cells / y_cells: ncells x SB^D, cell-major, local order of dof_map.
+ * Uses the cell quantities given to sf_set_cell_quantities (ncells must match
+ * unless they were given with fill = 1).
+ */
+int sf_evaluate_cells(sf_op* op, int dtype, int64_t ncells, const void* x_cells,
+                      void* y_cells, void* stream);
+
+/* diag(A) over the free dofs (device pointer of dtype), for Jacobi. */
+int sf_diagonal(sf_op* op, int dtype, void* d, void* stream);
+
+/*
+ * Conjugate gradients on A x = b, device FP64 pointers b and x (x is the
+ * initial guess on entry). Replaces IterativeSolvers.cg!(x, A, b) as called
+ * at profiling/drivers.jl:85-95. Stops when ||r||_2 <= reltol * ||b||_2
+ * (FP64 true residual for SF_CG_MIXED). Reports iterations (total inner
+ * iterations for SF_CG_MIXED) and the final relative residual.
+ */
+int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter,
+          int* iters, double* relres, void* stream);
+
+/*
+ * Named numeric options of a handle:
+ *   "mixed_inner_reltol" : inner FP32 CG relative tolerance of SF_CG_MIXED (default 1e-4)
+ *   "mixed_max_outer"    : cap on FP64 refinement steps of SF_CG_MIXED (default 50)
+ */
+int sf_set_option(sf_op* op, const char* name, double value);
+
+/* Outer (refinement) steps, inner iterations and relative residual of the last sf_cg. */
+int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
+
+/*
+ * Read-only facts about a handle, by name:
+ *   "n_free", "n_cells"      : sizes
+ *   "tiled_kernel"           : 1 if sf_apply(SF_F64) uses the tiled Cartesian kernel
+ *   "kernels_per_apply"      : kernel launches one sf_apply(SF_F64) makes
+ *   "geometry_kind"          : 1 separable constant metric, 2 per-point table
+ */
+int sf_get_info(const sf_op* op, const char* key, double* value);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SFB200_H */

@@ -1,0 +1,419 @@
+// General element kernel: one element per group of max(SB,SQ)^2 threads.
+//
+// This is the per-cell action Arrays.evaluate! of SumFactorizationMap
+// (src/SumFactorizationMaps.jl:78-89) together with the gather/assemble of
+// LazyMatrix mul! (src/LazyMatrices.jl:52-61). The arithmetic is the same
+// y_e = sum_r B_r^T G B_r x_e. The reference loops over D redundant
+// components (src/SumFactorizationKernels.jl:40-65,105-130). Here the
+// interpolation is shared between the gradient components instead:
+//   forward  x: A1 = A x, B1 = B x            (SB*SB lines)
+//            y: AA = A A1, AB = B A1, BA = A B1 (SQ*SB lines)
+//            z: ux = A BA, uy = A AB, uz = B AA (SQ*SQ lines, registers)
+//   metric   v = G(q) u, with G = wq djq jq^T jq (src/SumFactorizationKernels.jl:174-216)
+//   backward the transposes in reverse order.
+// Every pass gives each thread one full 1D line, read from shared memory into
+// registers. The thread computes all outputs of the line, so every value
+// loaded is reused SQ (or SB) times. The 1D matrices sit in the kernel's
+// __grid_constant__ parameters, so the FMAs take them straight from the
+// constant bank. The scatter-add uses atomics into a y that was zeroed before
+// the launch. Dirichlet dofs (id < 0) read as zero and are skipped.
+#include "sf_internal.cuh"
+
+namespace sf {
+namespace {
+
+template <int SB, int SQ, typename T>
+struct GenParams {
+  T A[SQ * SB];  // [qp][basis]
+  T B[SQ * SB];
+  double w1[SQ];
+  double G0[6];
+  const T* x;
+  T* y;
+  const int32_t* ids;   // CSR tensor-ordered ids or null (structured)
+  const int32_t* t2l;     // cell-local mode: tensor position -> local dof k
+  long long ncells;
+  int nx, ny, nz;
+  int mode;             // 0 = assembled apply, 1 = cell-local evaluate, 2 = diagonal
+  int geom;             // GEOM_SEPARABLE / GEOM_TABLE
+  const double* gtab;
+  long long gstride;
+  const double* kappa;
+};
+
+template <int SB, int SQ>
+struct Shape {
+  static constexpr int SM = SB > SQ ? SB : SQ;
+  static constexpr int NL = SM * SM;                    // threads per element
+  static constexpr int S0 = SB * SB * SB;                // X / Y
+  static constexpr int S1 = SB * SB * SQ;                // each of A1, B1
+  static constexpr int S2 = SB * SQ * SQ;                // each of AA, AB, BA
+  static constexpr int SE = S0 + 2 * S1 + 3 * S2;        // words per element
+  static constexpr int EPB = (256 / NL) > 0 ? (256 / NL) : 1;  // elements per block
+  static constexpr int THREADS = EPB * NL;
+};
+
+// Global free index of tensor position `pos` of cell `c` on the structured mesh, or -1.
+__device__ __forceinline__ long long structured_index(long long c, int pos, int SB, int nx, int ny,
+                                                      int nz) {
+  const int p = SB - 1;
+  const int cx = (int)(c % nx);
+  const long long r = c / nx;
+  const int cy = (int)(r % ny);
+  const int cz = (int)(r / ny);
+  const int i = pos % SB, j = (pos / SB) % SB, k = pos / (SB * SB);
+  const int gx = cx * p + i, gy = cy * p + j, gz = cz * p + k;
+  const int Nx = nx * p, Ny = ny * p, Nz = nz * p;
+  if (gx <= 0 || gx >= Nx || gy <= 0 || gy >= Ny || gz <= 0 || gz >= Nz) return -1;
+  return (long long)(gx - 1) + (long long)(Nx - 1) * ((long long)(gy - 1) + (long long)(Ny - 1) * (gz - 1));
+}
+
+template <typename T>
+__device__ __forceinline__ void atomic_add(T* a, T v) { atomicAdd(a, v); }
+
+template <int SB, int SQ, typename T>
+__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS)
+k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
+  using S = Shape<SB, SQ>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int el = threadIdx.x / S::NL;
+  const int l = threadIdx.x % S::NL;
+  const long long cell = (long long)blockIdx.x * S::EPB + el;
+  const bool valid = cell < P.ncells;
+
+  T* X = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SE;
+  T* A1 = X + S::S0;
+  T* B1 = A1 + S::S1;
+  T* AA = B1 + S::S1;
+  T* AB = AA + S::S2;
+  T* BA = AB + S::S2;
+
+  // ---------------- gather ----------------
+  for (int pos = l; pos < S::S0; pos += S::NL) {
+    T v = T(0);
+    if (valid) {
+      if (P.mode == 1) {
+        // cell-local: x_cells[cell][k] with k the local dof of tensor position pos
+        v = P.x[cell * S::S0 + P.t2l[pos]];
+      } else if (P.ids) {
+        const int id = P.ids[cell * S::S0 + pos];
+        if (id >= 0) v = P.x[id];
+      } else {
+        const long long id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+        if (id >= 0) v = P.x[id];
+      }
+    }
+    X[pos] = v;
+  }
+  __syncthreads();
+
+  // ---------------- forward x: lines (j,k), contract i ----------------
+  if (l < SB * SB) {
+    const int line = l;  // = j + SB*k
+    T in[SB];
+#pragma unroll
+    for (int i = 0; i < SB; ++i) in[i] = X[line * SB + i];
+#pragma unroll
+    for (int qi = 0; qi < SQ; ++qi) {
+      T a = T(0), b = T(0);
+#pragma unroll
+      for (int i = 0; i < SB; ++i) {
+        a = fma(P.A[qi * SB + i], in[i], a);
+        b = fma(P.B[qi * SB + i], in[i], b);
+      }
+      A1[line * SQ + qi] = a;
+      B1[line * SQ + qi] = b;
+    }
+  }
+  __syncthreads();
+
+  // ---------------- forward y: lines (qi,k), contract j ----------------
+  if (l < SQ * SB) {
+    const int qi = l % SQ, k = l / SQ;
+    T a1[SB], b1[SB];
+#pragma unroll
+    for (int j = 0; j < SB; ++j) {
+      a1[j] = A1[(k * SB + j) * SQ + qi];
+      b1[j] = B1[(k * SB + j) * SQ + qi];
+    }
+#pragma unroll
+    for (int qj = 0; qj < SQ; ++qj) {
+      T aa = T(0), ab = T(0), ba = T(0);
+#pragma unroll
+      for (int j = 0; j < SB; ++j) {
+        aa = fma(P.A[qj * SB + j], a1[j], aa);
+        ab = fma(P.B[qj * SB + j], a1[j], ab);
+        ba = fma(P.A[qj * SB + j], b1[j], ba);
+      }
+      const int o = (k * SQ + qj) * SQ + qi;
+      AA[o] = aa;
+      AB[o] = ab;
+      BA[o] = ba;
+    }
+  }
+  __syncthreads();
+
+  // ------- forward z, metric, backward z: lines (qi,qj), registers -------
+  if (l < SQ * SQ) {
+    const int qi = l % SQ, qj = l / SQ;
+    T ba[SB], ab[SB], aa[SB];
+#pragma unroll
+    for (int k = 0; k < SB; ++k) {
+      const int o = (k * SQ + qj) * SQ + qi;
+      ba[k] = BA[o];
+      ab[k] = AB[o];
+      aa[k] = AA[o];
+    }
+    T ba_o[SB], ab_o[SB], aa_o[SB];
+#pragma unroll
+    for (int k = 0; k < SB; ++k) ba_o[k] = ab_o[k] = aa_o[k] = T(0);
+#pragma unroll
+    for (int qk = 0; qk < SQ; ++qk) {
+      T ux = T(0), uy = T(0), uz = T(0);
+#pragma unroll
+      for (int k = 0; k < SB; ++k) {
+        ux = fma(P.A[qk * SB + k], ba[k], ux);
+        uy = fma(P.A[qk * SB + k], ab[k], uy);
+        uz = fma(P.B[qk * SB + k], aa[k], uz);
+      }
+      // metric in FP64 (geometric factors are kept in FP64 for both dtypes)
+      const int q = qi + SQ * (qj + SQ * qk);
+      double g[6];
+      if (P.geom == GEOM_SEPARABLE) {
+        const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) g[c] = s * P.G0[c];
+      } else {
+        const double* gt = P.gtab + (valid ? cell : 0) * P.gstride;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) g[c] = gt[c * SQ * SQ * SQ + q];
+      }
+      if (P.kappa) {
+        const double kq = valid ? P.kappa[cell * (SQ * SQ * SQ) + q] : 0.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) g[c] *= kq;
+      }
+      const double dx = (double)ux, dy = (double)uy, dz = (double)uz;
+      const T vx = (T)(g[0] * dx + g[3] * dy + g[4] * dz);
+      const T vy = (T)(g[3] * dx + g[1] * dy + g[5] * dz);
+      const T vz = (T)(g[4] * dx + g[5] * dy + g[2] * dz);
+#pragma unroll
+      for (int k = 0; k < SB; ++k) {
+        ba_o[k] = fma(P.A[qk * SB + k], vx, ba_o[k]);
+        ab_o[k] = fma(P.A[qk * SB + k], vy, ab_o[k]);
+        aa_o[k] = fma(P.B[qk * SB + k], vz, aa_o[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < SB; ++k) {
+      const int o = (k * SQ + qj) * SQ + qi;
+      BA[o] = ba_o[k];
+      AB[o] = ab_o[k];
+      AA[o] = aa_o[k];
+    }
+  }
+  __syncthreads();
+
+  // ---------------- backward y: lines (qi,k) ----------------
+  if (l < SQ * SB) {
+    const int qi = l % SQ, k = l / SQ;
+    T aa[SQ], ab[SQ], ba[SQ];
+#pragma unroll
+    for (int qj = 0; qj < SQ; ++qj) {
+      const int o = (k * SQ + qj) * SQ + qi;
+      aa[qj] = AA[o];
+      ab[qj] = AB[o];
+      ba[qj] = BA[o];
+    }
+#pragma unroll
+    for (int j = 0; j < SB; ++j) {
+      T a1 = T(0), b1 = T(0);
+#pragma unroll
+      for (int qj = 0; qj < SQ; ++qj) {
+        a1 = fma(P.A[qj * SB + j], aa[qj], a1);
+        a1 = fma(P.B[qj * SB + j], ab[qj], a1);
+        b1 = fma(P.A[qj * SB + j], ba[qj], b1);
+      }
+      A1[(k * SB + j) * SQ + qi] = a1;
+      B1[(k * SB + j) * SQ + qi] = b1;
+    }
+  }
+  __syncthreads();
+
+  // ---------------- backward x: lines (j,k) -> Y in X ----------------
+  if (l < SB * SB) {
+    const int line = l;
+    T a1[SQ], b1[SQ];
+#pragma unroll
+    for (int qi = 0; qi < SQ; ++qi) {
+      a1[qi] = A1[line * SQ + qi];
+      b1[qi] = B1[line * SQ + qi];
+    }
+#pragma unroll
+    for (int i = 0; i < SB; ++i) {
+      T yv = T(0);
+#pragma unroll
+      for (int qi = 0; qi < SQ; ++qi) {
+        yv = fma(P.A[qi * SB + i], a1[qi], yv);
+        yv = fma(P.B[qi * SB + i], b1[qi], yv);
+      }
+      X[line * SB + i] = yv;
+    }
+  }
+  __syncthreads();
+
+  // ---------------- scatter ----------------
+  if (!valid) return;
+  for (int pos = l; pos < S::S0; pos += S::NL) {
+    const T v = X[pos];
+    if (P.mode == 1) {
+      P.y[cell * S::S0 + P.t2l[pos]] = v;
+    } else if (P.ids) {
+      const int id = P.ids[cell * S::S0 + pos];
+      if (id >= 0) atomic_add(P.y + id, v);
+    } else {
+      const long long id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+      if (id >= 0) atomic_add(P.y + id, v);
+    }
+  }
+}
+
+// Diagonal of the assembled operator: for each cell and tensor position a,
+// diag_e[a] = sum_q sum_{r,s} G_rs(q) dphi_a/dxi_r(q) dphi_a/dxi_s(q), with the
+// 3D basis gradient a product of 1D values. One thread per (cell, a); the sum
+// over q is factorized into 1D sums when G is separable and diagonal, and
+// done point by point otherwise. Assembled with atomics (Jacobi needs diag(A)).
+template <int SB, int SQ, typename T>
+__global__ void k_general_diag(const __grid_constant__ GenParams<SB, SQ, T> P) {
+  constexpr int S0 = SB * SB * SB;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.ncells * S0) return;
+  const long long cell = t / S0;
+  const int pos = (int)(t % S0);
+  long long id;
+  if (P.ids) id = P.ids[cell * S0 + pos];
+  else id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+  if (id < 0) return;
+  const int a1 = pos % SB, a2 = (pos / SB) % SB, a3 = pos / (SB * SB);
+  double acc = 0.0;
+  for (int qk = 0; qk < SQ; ++qk)
+    for (int qj = 0; qj < SQ; ++qj)
+      for (int qi = 0; qi < SQ; ++qi) {
+        const int q = qi + SQ * (qj + SQ * qk);
+        const double Ax = (double)P.A[qi * SB + a1], Bx = (double)P.B[qi * SB + a1];
+        const double Ay = (double)P.A[qj * SB + a2], By = (double)P.B[qj * SB + a2];
+        const double Az = (double)P.A[qk * SB + a3], Bz = (double)P.B[qk * SB + a3];
+        const double gx = Bx * Ay * Az, gy = Ax * By * Az, gz = Ax * Ay * Bz;
+        double g[6];
+        if (P.geom == GEOM_SEPARABLE) {
+          const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
+          for (int c = 0; c < 6; ++c) g[c] = s * P.G0[c];
+        } else {
+          const double* gt = P.gtab + cell * P.gstride;
+          for (int c = 0; c < 6; ++c) g[c] = gt[c * SQ * SQ * SQ + q];
+        }
+        double kq = P.kappa ? P.kappa[cell * (SQ * SQ * SQ) + q] : 1.0;
+        acc += kq * (g[0] * gx * gx + g[1] * gy * gy + g[2] * gz * gz +
+                     2.0 * (g[3] * gx * gy + g[4] * gx * gz + g[5] * gy * gz));
+      }
+  atomicAdd(P.y + id, (T)acc);
+}
+
+template <int SB, int SQ, typename T>
+GenParams<SB, SQ, T> make_params(const double* A, const double* B, const Geometry& geom) {
+  GenParams<SB, SQ, T> P{};
+  for (int i = 0; i < SQ * SB; ++i) {
+    P.A[i] = (T)A[i];
+    P.B[i] = (T)B[i];
+  }
+  for (int i = 0; i < SQ; ++i) P.w1[i] = geom.w1[i];
+  for (int c = 0; c < 6; ++c) P.G0[c] = geom.G0[c];
+  P.geom = geom.kind;
+  P.gtab = geom.table;
+  P.gstride = geom.table_stride;
+  P.kappa = geom.kappa;
+  return P;
+}
+
+template <int SB, int SQ, typename T>
+void run_general(int mode, const double* A, const double* B, const Cells& cells,
+                 long long ncells, const int32_t* t2l, const Geometry& geom, const void* x,
+                 void* y, cudaStream_t stream) {
+  using S = Shape<SB, SQ>;
+  auto P = make_params<SB, SQ, T>(A, B, geom);
+  P.x = static_cast<const T*>(x);
+  P.y = static_cast<T*>(y);
+  P.ids = cells.ids;
+  P.t2l = t2l;
+  P.ncells = ncells;
+  P.nx = cells.nx;
+  P.ny = cells.ny;
+  P.nz = cells.nz;
+  P.mode = mode;
+  if (ncells == 0) return;
+  if (mode == 2) {
+    const long long total = ncells * S::S0;
+    const int threads = 256;
+    const long long blocks = (total + threads - 1) / threads;
+    k_general_diag<SB, SQ, T><<<(unsigned)blocks, threads, 0, stream>>>(P);
+    SF_CUDA_CHECK(cudaGetLastError());
+    return;
+  }
+  const size_t smem = (size_t)S::EPB * S::SE * sizeof(T);
+  SF_CUDA_CHECK(cudaFuncSetAttribute(k_general<SB, SQ, T>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long blocks = (ncells + S::EPB - 1) / S::EPB;
+  SF_REQUIRE(blocks < (1LL << 31), SF_ERR_ARG, "too many cells for one launch");
+  k_general<SB, SQ, T><<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+using RunFn = void (*)(int, const double*, const double*, const Cells&, long long, const int32_t*,
+                       const Geometry&, const void*, void*, cudaStream_t);
+
+// Instantiated (SB, SQ) pairs: SB = 2..10, SQ in SB-1..SB+2 (1..10).
+template <typename T>
+RunFn select(int SB, int SQ) {
+#define SF_CASE(sb, sq) \
+  if (SB == sb && SQ == sq) return &run_general<sb, sq, T>;
+#define SF_ROW(sb) SF_CASE(sb, sb - 1) SF_CASE(sb, sb) SF_CASE(sb, sb + 1) SF_CASE(sb, sb + 2)
+  SF_ROW(2) SF_ROW(3) SF_ROW(4) SF_ROW(5) SF_ROW(6) SF_ROW(7) SF_ROW(8)
+  SF_CASE(9, 8) SF_CASE(9, 9) SF_CASE(9, 10)
+  SF_CASE(10, 9) SF_CASE(10, 10)
+#undef SF_ROW
+#undef SF_CASE
+  return nullptr;
+}
+
+RunFn select_dtype(int dtype, int SB, int SQ) {
+  RunFn f = nullptr;
+  if (dtype == SF_F64) f = select<double>(SB, SQ);
+  else if (dtype == SF_F32) f = select<float>(SB, SQ);
+  else throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
+  if (!f)
+    throw Error(SF_ERR_UNSUPPORTED, "no general kernel instantiated for SB=" + std::to_string(SB) +
+                                        " SQ=" + std::to_string(SQ));
+  return f;
+}
+
+}  // namespace
+
+void launch_general_apply(int dtype, int SB, int SQ, const double* A, const double* B,
+                          const Cells& cells, const Geometry& geom, const void* x, void* y,
+                          cudaStream_t stream) {
+  select_dtype(dtype, SB, SQ)(0, A, B, cells, cells.ncells, nullptr, geom, x, y, stream);
+}
+
+void launch_general_diag(int dtype, int SB, int SQ, const double* A, const double* B,
+                         const Cells& cells, const Geometry& geom, void* d, cudaStream_t stream) {
+  select_dtype(dtype, SB, SQ)(2, A, B, cells, cells.ncells, nullptr, geom, nullptr, d, stream);
+}
+
+void launch_general_evaluate(int dtype, int SB, int SQ, const double* A, const double* B,
+                             long long ncells, const int32_t* t2l, const Geometry& geom,
+                             const void* x_cells, void* y_cells, cudaStream_t stream) {
+  Cells none;
+  select_dtype(dtype, SB, SQ)(1, A, B, none, ncells, t2l, geom, x_cells, y_cells, stream);
+}
+
+}  // namespace sf

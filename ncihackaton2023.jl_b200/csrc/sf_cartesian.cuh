@@ -1,0 +1,26 @@
+// Tiled Cartesian kernels (kernels_cartesian.cu): constant-coefficient
+// axis-aligned affine cells on a structured mesh.
+#pragma once
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+struct CartesianPlan {
+  bool ready = false;
+  int SB = 0, SQ = 0, nx = 0, ny = 0, nz = 0;
+  double M[kMaxSB * kMaxSB] = {0};  // 1D element mass A^T W A, lexicographic order
+  double K[kMaxSB * kMaxSB] = {0};  // 1D element stiffness B^T W B
+  double c[3] = {0, 0, 0};          // G0 diagonal: xx, yy, zz
+};
+
+// Builds the 1D operators; returns false when no tiled kernel exists for SB.
+bool cartesian_prepare(CartesianPlan& plan, int SB, int SQ, const double* A, const double* B,
+                       const double* w1, const double* G0, int nx, int ny, int nz);
+bool cartesian_supported(const CartesianPlan& plan, int dtype);
+int cartesian_launches(const CartesianPlan& plan);  // kernel launches per apply
+void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
+                     cudaStream_t stream);
+void cartesian_release(CartesianPlan& plan);
+
+}  // namespace sf

@@ -1,0 +1,71 @@
+// Internal declarations shared by the sfb200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sfb200.h"
+
+namespace sf {
+
+constexpr int kMaxSB = 10;
+constexpr int kMaxSQ = 10;
+
+enum MeshKind { MESH_NONE = 0, MESH_CSR = 1, MESH_STRUCTURED = 2 };
+enum GeomKind { GEOM_NONE = 0, GEOM_SEPARABLE = 1, GEOM_TABLE = 2 };
+
+// Error carried from the internals to the ABI layer.
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define SF_CUDA_CHECK(expr)                                                              \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      throw ::sf::Error(SF_ERR_CUDA, std::string(#expr " failed: ") + cudaGetErrorString(_e)); \
+  } while (0)
+
+#define SF_REQUIRE(cond, status, msg)                   \
+  do {                                                  \
+    if (!(cond)) throw ::sf::Error((status), (msg));    \
+  } while (0)
+
+// Device geometry shared by the element kernels.
+struct Geometry {
+  int kind = GEOM_NONE;
+  double w1[kMaxSQ] = {0};   // separable: 1D weights, G(q) = w_i w_j w_k G0
+  double G0[6] = {0};        // xx, yy, zz, xy, xz, yz
+  const double* table = nullptr;  // table: [cell][6][SQ^3]
+  long long table_stride = 0;     // doubles per cell (0 = one cell shared by all)
+  const double* kappa = nullptr;  // [cell][SQ^3] or null
+};
+
+// Gather/scatter description shared by the element kernels.
+struct Cells {
+  int mesh = MESH_NONE;
+  long long ncells = 0;
+  const int32_t* ids = nullptr;  // CSR: [cell][SB^3] tensor order, 0-based free id or -1
+  int nx = 0, ny = 0, nz = 0;    // structured
+  int p = 0;
+};
+
+// Launchers implemented in kernels_general.cu. A, B: SQ x SB row-major
+// ([qp][basis]) in the kernel's 1D order.
+void launch_general_apply(int dtype, int SB, int SQ, const double* A, const double* B,
+                          const Cells& cells, const Geometry& geom, const void* x, void* y,
+                          cudaStream_t stream);
+void launch_general_diag(int dtype, int SB, int SQ, const double* A, const double* B,
+                         const Cells& cells, const Geometry& geom, void* d, cudaStream_t stream);
+// Cell-local evaluation: x_cells/y_cells [cell][SB^3] in local order; t2l (device) maps
+// tensor position -> local dof.
+void launch_general_evaluate(int dtype, int SB, int SQ, const double* A, const double* B,
+                             long long ncells, const int32_t* t2l, const Geometry& geom,
+                             const void* x_cells, void* y_cells, cudaStream_t stream);
+
+}  // namespace sf

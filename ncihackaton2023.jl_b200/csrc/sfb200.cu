@@ -1,0 +1,685 @@
+// C ABI of the sum-factorized Laplacian operator (include/sfb200.h).
+//
+// The handle mirrors the pair SumFactorizationMap + LazyMatrix of the
+// reference (src/SumFactorizationMaps.jl:2-10, src/LazyMatrices.jl:1-50).
+// It owns the device copies of the 1D basis, the cell-to-dof table and the
+// geometric factors. The x and y vectors are borrowed from the caller.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "sf_cg.cuh"
+#include "sf_internal.cuh"
+#include "sf_cartesian.cuh"
+
+using sf::Error;
+
+struct sf_op {
+  int D = 3, SB = 0, SQ = 0, p = 0;
+  std::vector<double> A_user, B_user;  // [q][j], caller's 1D order
+  std::vector<int> jt_user;            // [k][d]: 0-based 1D index of local dof k along d
+  std::vector<int> perm;               // caller 1D index -> kernel 1D index
+  std::vector<double> A, B;            // [q][j], kernel 1D order
+  sf::Cells cells;
+  long long n_free = 0;
+  int32_t* d_ids = nullptr;
+  int32_t* d_t2l = nullptr;
+  sf::Geometry geom;
+  double* d_gtab = nullptr;
+  double* d_kappa = nullptr;
+  long long cq_cells = -1;  // -1 = unset, 0 = fill (one cell for all)
+  bool cartesian_ok = false;
+  sf::CartesianPlan cart;   // tiled Cartesian kernel set-up
+  // workspaces
+  double* d_diag = nullptr;  // FP64 diag(A), cached
+  void* d_ws = nullptr;
+  size_t ws_bytes = 0;
+  double* d_hx = nullptr;    // sf_mul_host staging
+  double* d_hy = nullptr;
+  double* h_scalar = nullptr;  // pinned
+  double mixed_inner_reltol = 1e-4;
+  int mixed_max_outer = 50;
+  int last_outer = 0, last_inner = 0;
+  double last_relres = 0.0;
+  std::string err;
+};
+
+namespace {
+
+int fail(sf_op* op, int status, const std::string& msg) {
+  if (op) op->err = msg;
+  return status;
+}
+
+template <typename F>
+int guarded(sf_op* op, F&& f) {
+  try {
+    f();
+    if (op) op->err.clear();
+    return SF_OK;
+  } catch (const Error& e) {
+    return fail(op, e.status, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(op, SF_ERR_ARG, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(op, SF_ERR_ARG, e.what());
+  }
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+template <typename T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  SF_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  return static_cast<T*>(p);
+}
+
+size_t dsize(int dtype) {
+  if (dtype == SF_F64) return 8;
+  if (dtype == SF_F32) return 4;
+  throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
+}
+
+// Kernel-order tensor position of local dof k.
+int tensor_pos(const sf_op* op, int k) {
+  int pos = 0, stride = 1;
+  for (int d = 0; d < op->D; ++d) {
+    pos += op->perm[op->jt_user[k * op->D + d]] * stride;
+    stride *= op->SB;
+  }
+  return pos;
+}
+
+void rebuild_kernel_basis(sf_op* op) {
+  const int SB = op->SB, SQ = op->SQ;
+  op->A.assign(SQ * SB, 0.0);
+  op->B.assign(SQ * SB, 0.0);
+  for (int q = 0; q < SQ; ++q)
+    for (int j = 0; j < SB; ++j) {
+      op->A[q * SB + op->perm[j]] = op->A_user[q * SB + j];
+      op->B[q * SB + op->perm[j]] = op->B_user[q * SB + j];
+    }
+  const int nloc = SB * SB * SB;
+  std::vector<int32_t> t2l(nloc, -1);
+  for (int k = 0; k < nloc; ++k) t2l[tensor_pos(op, k)] = k;
+  for (int v : t2l)
+    SF_REQUIRE(v >= 0, SF_ERR_ARG, "dof_map is not a permutation of the tensor indices");
+  dfree(op->d_t2l);
+  op->d_t2l = nullptr;
+  op->d_t2l = dalloc<int32_t>(nloc);
+  SF_CUDA_CHECK(cudaMemcpy(op->d_t2l, t2l.data(), nloc * sizeof(int32_t), cudaMemcpyHostToDevice));
+}
+
+void require_ready(const sf_op* op) {
+  SF_REQUIRE(op, SF_ERR_ARG, "null handle");
+  SF_REQUIRE(op->cells.mesh != sf::MESH_NONE, SF_ERR_STATE,
+             "no mesh: call sf_set_cells or sf_set_structured first");
+  SF_REQUIRE(op->geom.kind != sf::GEOM_NONE, SF_ERR_STATE,
+             "no geometry: call sf_set_cell_quantities first");
+  SF_REQUIRE(op->cq_cells == 0 || op->cq_cells == op->cells.ncells, SF_ERR_STATE,
+             "cell quantities were given for a different number of cells");
+}
+
+void update_cartesian(sf_op* op) {
+  op->cartesian_ok = false;
+  if (op->cells.mesh != sf::MESH_STRUCTURED || op->geom.kind != sf::GEOM_SEPARABLE ||
+      op->geom.kappa != nullptr)
+    return;
+  const double* G = op->geom.G0;
+  const double scale = std::max({std::fabs(G[0]), std::fabs(G[1]), std::fabs(G[2])});
+  if (std::fabs(G[3]) > 1e-14 * scale || std::fabs(G[4]) > 1e-14 * scale ||
+      std::fabs(G[5]) > 1e-14 * scale)
+    return;
+  op->cartesian_ok = sf::cartesian_prepare(op->cart, op->SB, op->SQ, op->A.data(), op->B.data(),
+                                           op->geom.w1, G, op->cells.nx, op->cells.ny,
+                                           op->cells.nz);
+}
+
+void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
+  require_ready(op);
+  const size_t es = dsize(dtype);
+  if (op->n_free == 0) return;
+  SF_REQUIRE(x && y, SF_ERR_ARG, "null x or y");
+  SF_REQUIRE(x != y, SF_ERR_ARG, "x and y must not alias");
+  if (op->cartesian_ok && sf::cartesian_supported(op->cart, dtype)) {
+    sf::cartesian_apply(op->cart, dtype, x, y, st);
+    return;
+  }
+  SF_CUDA_CHECK(cudaMemsetAsync(y, 0, op->n_free * es, st));
+  sf::launch_general_apply(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
+                           x, y, st);
+}
+
+void ensure_diag(sf_op* op, cudaStream_t st) {
+  if (op->d_diag) return;
+  op->d_diag = dalloc<double>(op->n_free);
+  SF_CUDA_CHECK(cudaMemsetAsync(op->d_diag, 0, op->n_free * sizeof(double), st));
+  sf::launch_general_diag(SF_F64, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
+                          op->d_diag, st);
+}
+
+void invalidate_caches(sf_op* op) {
+  dfree(op->d_diag);
+  op->d_diag = nullptr;
+}
+
+void* workspace(sf_op* op, size_t bytes) {
+  if (op->ws_bytes < bytes) {
+    dfree(op->d_ws);
+    op->d_ws = nullptr;
+    op->ws_bytes = 0;
+    SF_CUDA_CHECK(cudaMalloc(&op->d_ws, bytes));
+    op->ws_bytes = bytes;
+  }
+  return op->d_ws;
+}
+
+double read_scalar(sf_op* op, const double* d_s, int slot, cudaStream_t st) {
+  if (!op->h_scalar) SF_CUDA_CHECK(cudaMallocHost(&op->h_scalar, 8 * sizeof(double)));
+  SF_CUDA_CHECK(cudaMemcpyAsync(op->h_scalar, d_s + slot, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SF_CUDA_CHECK(cudaStreamSynchronize(st));
+  return op->h_scalar[0];
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Plain or Jacobi FP64 CG. Returns iterations; sets relres.
+int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, int maxiter,
+           double* relres, cudaStream_t st) {
+  const long long n = op->n_free;
+  const size_t vb = align256(n * sizeof(double));
+  const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
+  const size_t pb = align256(sf::kRedBlocks * 3 * sizeof(double));
+  char* ws = static_cast<char*>(workspace(op, 4 * vb + sb + pb));
+  double* r = reinterpret_cast<double*>(ws);
+  double* p = reinterpret_cast<double*>(ws + vb);
+  double* q = reinterpret_cast<double*>(ws + 2 * vb);
+  double* dinv = reinterpret_cast<double*>(ws + 3 * vb);
+  double* s = reinterpret_cast<double*>(ws + 4 * vb);
+  double* partials = reinterpret_cast<double*>(ws + 4 * vb + sb);
+  if (jacobi) {
+    ensure_diag(op, st);
+    sf::vec_invert<double>(op->d_diag, dinv, n, st);
+  }
+  const double* Dv = jacobi ? dinv : nullptr;
+  apply_impl(op, SF_F64, x, q, st);
+  sf::cg_start<double>(b, q, Dv, r, p, n, partials, s, st);
+  double bb = read_scalar(op, s, sf::CG_BB, st);
+  double rr = read_scalar(op, s, sf::CG_RR, st);
+  const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
+  const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
+  int it = 0;
+  while (rr > tol2 && it < maxiter) {
+    apply_impl(op, SF_F64, p, q, st);
+    sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, st);
+    sf::cg_update<double>(s, x, p, r, q, Dv, n, partials, s, st);
+    rr = read_scalar(op, s, sf::CG_RR, st);
+    ++it;
+    SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in CG");
+    if (rr <= tol2) break;
+    sf::cg_direction<double>(s, p, r, Dv, n, st);
+  }
+  *relres = std::sqrt(rr) / nb;
+  return it;
+}
+
+// FP32 apply + FP32 inner Jacobi CG with FP64 dots; FP64 outer refinement.
+int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, double* relres,
+             int* outer_out, cudaStream_t st) {
+  const long long n = op->n_free;
+  const size_t v8 = align256(n * sizeof(double));
+  const size_t v4 = align256(n * sizeof(float));
+  const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
+  const size_t pb = align256(sf::kRedBlocks * 3 * sizeof(double));
+  char* ws = static_cast<char*>(workspace(op, 2 * v8 + 6 * v4 + sb + pb));
+  double* r64 = reinterpret_cast<double*>(ws);
+  double* q64 = reinterpret_cast<double*>(ws + v8);
+  char* w4 = ws + 2 * v8;
+  float* rhs32 = reinterpret_cast<float*>(w4);
+  float* d32 = reinterpret_cast<float*>(w4 + v4);
+  float* r32 = reinterpret_cast<float*>(w4 + 2 * v4);
+  float* p32 = reinterpret_cast<float*>(w4 + 3 * v4);
+  float* q32 = reinterpret_cast<float*>(w4 + 4 * v4);
+  float* dinv32 = reinterpret_cast<float*>(w4 + 5 * v4);
+  double* s = reinterpret_cast<double*>(ws + 2 * v8 + 6 * v4);
+  double* partials = reinterpret_cast<double*>(ws + 2 * v8 + 6 * v4 + sb);
+  ensure_diag(op, st);
+  sf::vec_invert<float>(op->d_diag, dinv32, n, st);
+  // ||b||
+  sf::vec_dot<double>(b, b, n, partials, s + sf::CG_BB, st);
+  const double bb = read_scalar(op, s, sf::CG_BB, st);
+  const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
+  const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
+  const double eta2 = op->mixed_inner_reltol * op->mixed_inner_reltol;
+  int inner_total = 0, outer = 0;
+  double rr64 = 0.0;
+  for (;;) {
+    apply_impl(op, SF_F64, x, q64, st);
+    sf::mixed_residual(b, q64, r64, n, partials, s, sf::CG_RES64, st);
+    rr64 = read_scalar(op, s, sf::CG_RES64, st);
+    SF_REQUIRE(std::isfinite(rr64), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
+    if (rr64 <= tol2 || inner_total >= maxiter || outer >= op->mixed_max_outer) break;
+    ++outer;
+    sf::mixed_scale(s, sf::CG_RES64, r64, rhs32, d32, n, st);
+    // inner CG from d = 0 on A d = rhs32 (||rhs32|| = 1)
+    sf::cg_start<float>(rhs32, nullptr, dinv32, r32, p32, n, partials, s, st);
+    double rr = read_scalar(op, s, sf::CG_RR, st);
+    const double itol2 = eta2 * rr;
+    int it = 0;
+    while (rr > itol2 && inner_total < maxiter) {
+      apply_impl(op, SF_F32, p32, q32, st);
+      sf::vec_dot<float>(p32, q32, n, partials, s + sf::CG_PQ, st);
+      sf::cg_update<float>(s, d32, p32, r32, q32, dinv32, n, partials, s, st);
+      rr = read_scalar(op, s, sf::CG_RR, st);
+      ++it;
+      ++inner_total;
+      SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in inner CG");
+      if (rr <= itol2) break;
+      sf::cg_direction<float>(s, p32, r32, dinv32, n, st);
+    }
+    sf::mixed_correct(s, sf::CG_RES64, x, d32, n, st);
+  }
+  *relres = std::sqrt(rr64) / nb;
+  *outer_out = outer;
+  return inner_total;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sf_version(void) { return 100; }
+
+const char* sf_status_string(int status) {
+  switch (status) {
+    case SF_OK: return "ok";
+    case SF_ERR_ARG: return "invalid argument";
+    case SF_ERR_CUDA: return "CUDA error";
+    case SF_ERR_STATE: return "handle not set up";
+    case SF_ERR_UNSUPPORTED: return "unsupported";
+    case SF_ERR_NOT_CONVERGED: return "not converged";
+    case SF_ERR_NONFINITE: return "non-finite value";
+    default: return "unknown status";
+  }
+}
+
+int sf_create(sf_op** out, int D, int SB, int SQ, const double* A0, const double* B0,
+              const int32_t* dof_map) {
+  if (!out) return SF_ERR_ARG;
+  *out = nullptr;
+  if (D == 2) return SF_ERR_UNSUPPORTED;
+  if (D != 3 || SB < 2 || SB > sf::kMaxSB || SQ < 1 || SQ > sf::kMaxSQ || !A0 || !B0 || !dof_map)
+    return SF_ERR_ARG;
+  sf_op* op = new (std::nothrow) sf_op();
+  if (!op) return SF_ERR_ARG;
+  op->D = D;
+  op->SB = SB;
+  op->SQ = SQ;
+  op->p = SB - 1;
+  op->A_user.resize(SQ * SB);
+  op->B_user.resize(SQ * SB);
+  for (int q = 0; q < SQ; ++q)
+    for (int j = 0; j < SB; ++j) {
+      op->A_user[q * SB + j] = A0[q + SQ * j];  // column-major in
+      op->B_user[q * SB + j] = B0[q + SQ * j];
+    }
+  const int nloc = SB * SB * SB;
+  op->jt_user.resize(nloc * D);
+  for (int k = 0; k < nloc; ++k)
+    for (int d = 0; d < D; ++d) {
+      const int v = dof_map[k + nloc * d] - 1;  // column-major, 1-based
+      if (v < 0 || v >= SB) {
+        delete op;
+        return SF_ERR_ARG;
+      }
+      op->jt_user[k * D + d] = v;
+    }
+  op->perm.resize(SB);
+  for (int j = 0; j < SB; ++j) op->perm[j] = j;
+  int st = guarded(op, [&] { rebuild_kernel_basis(op); });
+  if (st != SF_OK) {
+    sf_destroy(op);
+    return st;
+  }
+  *out = op;
+  return SF_OK;
+}
+
+int sf_destroy(sf_op* op) {
+  if (!op) return SF_OK;
+  dfree(op->d_ids);
+  dfree(op->d_t2l);
+  dfree(op->d_gtab);
+  dfree(op->d_kappa);
+  dfree(op->d_diag);
+  dfree(op->d_ws);
+  dfree(op->d_hx);
+  dfree(op->d_hy);
+  if (op->h_scalar) cudaFreeHost(op->h_scalar);
+  sf::cartesian_release(op->cart);
+  delete op;
+  return SF_OK;
+}
+
+const char* sf_last_error(const sf_op* op) { return op ? op->err.c_str() : "null handle"; }
+
+int sf_get_dimensional_parameters(const sf_op* op, int* D, int* SB, int* SQ) {
+  if (!op) return SF_ERR_ARG;
+  if (D) *D = op->D;
+  if (SB) *SB = op->SB;
+  if (SQ) *SQ = op->SQ;
+  return SF_OK;
+}
+
+int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* data,
+                 int64_t n_free) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(ncells >= 0 && n_free >= 0 && (ncells == 0 || (ptrs && data)), SF_ERR_ARG,
+               "bad arguments to sf_set_cells");
+    SF_REQUIRE(n_free < (1LL << 31), SF_ERR_ARG, "n_free must fit in int32");
+    const int nloc = op->SB * op->SB * op->SB;
+    for (int j = 0; j < op->SB; ++j) op->perm[j] = j;
+    rebuild_kernel_basis(op);
+    std::vector<int> tpos(nloc);
+    for (int k = 0; k < nloc; ++k) tpos[k] = tensor_pos(op, k);
+    std::vector<int32_t> ids((size_t)ncells * nloc);
+    for (int64_t c = 0; c < ncells; ++c) {
+      const int64_t b = (int64_t)ptrs[c] - 1, e = (int64_t)ptrs[c + 1] - 1;
+      SF_REQUIRE(e - b == nloc, SF_ERR_ARG,
+                 "cell " + std::to_string(c + 1) + " does not have SB^D dofs");
+      for (int k = 0; k < nloc; ++k) {
+        const int32_t id = data[b + k];
+        SF_REQUIRE(id != 0 && id <= n_free, SF_ERR_ARG,
+                   "dof id out of range in cell " + std::to_string(c + 1));
+        ids[(size_t)c * nloc + tpos[k]] = id > 0 ? id - 1 : -1;
+      }
+    }
+    dfree(op->d_ids);
+    op->d_ids = nullptr;
+    op->d_ids = dalloc<int32_t>(ids.size());
+    SF_CUDA_CHECK(cudaMemcpy(op->d_ids, ids.data(), ids.size() * sizeof(int32_t),
+                             cudaMemcpyHostToDevice));
+    op->cells = sf::Cells();
+    op->cells.mesh = sf::MESH_CSR;
+    op->cells.ncells = ncells;
+    op->cells.ids = op->d_ids;
+    op->cells.p = op->p;
+    op->n_free = n_free;
+    invalidate_caches(op);
+    update_cartesian(op);
+  });
+}
+
+int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_order) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(nx > 0 && ny > 0 && nz > 0 && node_order, SF_ERR_ARG,
+               "bad arguments to sf_set_structured");
+    std::vector<int> seen(op->SB, 0);
+    for (int j = 0; j < op->SB; ++j) {
+      SF_REQUIRE(node_order[j] >= 0 && node_order[j] < op->SB && !seen[node_order[j]], SF_ERR_ARG,
+                 "node_order must be a permutation of 0..p");
+      seen[node_order[j]] = 1;
+    }
+    const long long p = op->p;
+    const long long fx = nx * p - 1, fy = ny * p - 1, fz = nz * p - 1;
+    SF_REQUIRE(fx * fy * fz < (1LL << 31), SF_ERR_ARG, "mesh too large for int32 dof ids");
+    for (int j = 0; j < op->SB; ++j) op->perm[j] = node_order[j];
+    rebuild_kernel_basis(op);
+    dfree(op->d_ids);
+    op->d_ids = nullptr;
+    op->cells = sf::Cells();
+    op->cells.mesh = sf::MESH_STRUCTURED;
+    op->cells.ncells = (long long)nx * ny * nz;
+    op->cells.nx = nx;
+    op->cells.ny = ny;
+    op->cells.nz = nz;
+    op->cells.p = op->p;
+    op->n_free = fx * fy * fz;
+    invalidate_caches(op);
+    update_cartesian(op);
+  });
+}
+
+int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* jq,
+                           const double* djq) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(wq && jq && djq, SF_ERR_ARG, "null cell quantity");
+    SF_REQUIRE(fill || op->cells.mesh != sf::MESH_NONE, SF_ERR_STATE,
+               "per-cell quantities need the mesh first (sf_set_cells / sf_set_structured)");
+    const int SQ = op->SQ, D = op->D;
+    const int nq = SQ * SQ * SQ;
+    const long long nc = fill ? 1 : op->cells.ncells;
+    // G = wq*djq*jq^T jq at every point (src/SumFactorizationKernels.jl:174-216)
+    std::vector<double> G((size_t)nc * 6 * nq);
+    std::vector<double> H((size_t)nc * 6 * nq);  // djq*jq^T jq (without the weight)
+    static const int rr[6] = {0, 1, 2, 0, 0, 1}, kk[6] = {0, 1, 2, 1, 2, 2};
+    for (long long c = 0; c < nc; ++c)
+      for (int q = 0; q < nq; ++q) {
+        const double* J = jq + ((size_t)c * nq + q) * D * D;
+        const double w = wq[(size_t)c * nq + q], dj = djq[(size_t)c * nq + q];
+        for (int m = 0; m < 6; ++m) {
+          double acc = 0.0;
+          for (int l = 0; l < D; ++l) acc += J[l + D * rr[m]] * J[l + D * kk[m]];
+          H[((size_t)c * 6 + m) * nq + q] = dj * acc;
+          G[((size_t)c * 6 + m) * nq + q] = w * dj * acc;
+        }
+      }
+    // all cells equal?
+    bool same = true;
+    for (long long c = 1; c < nc && same; ++c)
+      for (size_t i = 0; i < (size_t)6 * nq; ++i)
+        if (G[(size_t)c * 6 * nq + i] != G[i]) {
+          same = false;
+          break;
+        }
+    // separable: H constant over points and wq a tensor product of 1D weights
+    bool sep = same;
+    double Hmax = 0.0;
+    for (int m = 0; m < 6; ++m) Hmax = std::max(Hmax, std::fabs(H[(size_t)m * nq]));
+    for (int m = 0; m < 6 && sep; ++m)
+      for (int q = 1; q < nq; ++q)
+        if (std::fabs(H[(size_t)m * nq + q] - H[(size_t)m * nq]) > 1e-13 * Hmax) {
+          sep = false;
+          break;
+        }
+    double w1[sf::kMaxSQ] = {0};
+    if (sep) {
+      const double w000 = wq[0];
+      sep = w000 > 0;
+      if (sep) {
+        const double c0 = std::cbrt(w000);
+        for (int i = 0; i < SQ; ++i) w1[i] = wq[i] / (c0 * c0);
+        for (int k = 0; k < SQ && sep; ++k)
+          for (int j = 0; j < SQ && sep; ++j)
+            for (int i = 0; i < SQ; ++i) {
+              const double t = w1[i] * w1[j] * w1[k];
+              if (std::fabs(t - wq[i + SQ * (j + SQ * k)]) > 1e-13 * std::fabs(t)) {
+                sep = false;
+                break;
+              }
+            }
+      }
+    }
+    dfree(op->d_gtab);
+    op->d_gtab = nullptr;
+    sf::Geometry g;
+    g.kappa = op->d_kappa;
+    if (sep) {
+      g.kind = sf::GEOM_SEPARABLE;
+      for (int i = 0; i < SQ; ++i) g.w1[i] = w1[i];
+      for (int m = 0; m < 6; ++m) g.G0[m] = H[(size_t)m * nq];
+    } else {
+      const long long ncopy = same ? 1 : nc;
+      op->d_gtab = dalloc<double>((size_t)ncopy * 6 * nq);
+      SF_CUDA_CHECK(cudaMemcpy(op->d_gtab, G.data(), (size_t)ncopy * 6 * nq * sizeof(double),
+                               cudaMemcpyHostToDevice));
+      g.kind = sf::GEOM_TABLE;
+      g.table = op->d_gtab;
+      g.table_stride = same ? 0 : 6LL * nq;
+    }
+    op->geom = g;
+    op->cq_cells = (fill || same) ? 0 : nc;
+    invalidate_caches(op);
+    update_cartesian(op);
+  });
+}
+
+int sf_set_coefficient(sf_op* op, const double* kappa) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    dfree(op->d_kappa);
+    op->d_kappa = nullptr;
+    if (kappa) {
+      SF_REQUIRE(op->cells.mesh != sf::MESH_NONE, SF_ERR_STATE, "set the mesh before kappa");
+      const size_t n = (size_t)op->cells.ncells * op->SQ * op->SQ * op->SQ;
+      op->d_kappa = dalloc<double>(n);
+      SF_CUDA_CHECK(cudaMemcpy(op->d_kappa, kappa, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    op->geom.kappa = op->d_kappa;
+    invalidate_caches(op);
+    update_cartesian(op);
+  });
+}
+
+int sf_apply(sf_op* op, int dtype, const void* x, void* y, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] { apply_impl(op, dtype, x, y, static_cast<cudaStream_t>(stream)); });
+}
+
+int sf_apply_multi(sf_op* op, int dtype, int nrhs, const void* x, int64_t ldx, void* y,
+                   int64_t ldy, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(nrhs >= 0 && ldx >= op->n_free && ldy >= op->n_free, SF_ERR_ARG,
+               "bad nrhs / leading dimensions");
+    const size_t es = dsize(dtype);
+    for (int k = 0; k < nrhs; ++k)
+      apply_impl(op, dtype, static_cast<const char*>(x) + (size_t)k * ldx * es,
+                 static_cast<char*>(y) + (size_t)k * ldy * es, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int sf_mul_host(sf_op* op, const double* x, double* y) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(x && y, SF_ERR_ARG, "null x or y");
+    const size_t bytes = op->n_free * sizeof(double);
+    if (!op->d_hx) {
+      op->d_hx = dalloc<double>(op->n_free);
+      op->d_hy = dalloc<double>(op->n_free);
+    }
+    cudaStream_t st = 0;
+    SF_CUDA_CHECK(cudaMemcpyAsync(op->d_hx, x, bytes, cudaMemcpyHostToDevice, st));
+    apply_impl(op, SF_F64, op->d_hx, op->d_hy, st);
+    SF_CUDA_CHECK(cudaMemcpyAsync(y, op->d_hy, bytes, cudaMemcpyDeviceToHost, st));
+    SF_CUDA_CHECK(cudaStreamSynchronize(st));
+  });
+}
+
+int sf_evaluate_cells(sf_op* op, int dtype, int64_t ncells, const void* x_cells, void* y_cells,
+                      void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(op->geom.kind != sf::GEOM_NONE, SF_ERR_STATE, "no geometry");
+    SF_REQUIRE(ncells >= 0, SF_ERR_ARG, "ncells < 0");
+    SF_REQUIRE(op->cq_cells <= 0 || op->cq_cells == ncells, SF_ERR_ARG,
+               "ncells differs from the cell quantities");
+    SF_REQUIRE(op->geom.kappa == nullptr || ncells == op->cells.ncells, SF_ERR_ARG,
+               "ncells differs from the coefficient field");
+    if (ncells == 0) return;
+    SF_REQUIRE(x_cells && y_cells, SF_ERR_ARG, "null x_cells or y_cells");
+    sf::launch_general_evaluate(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), ncells,
+                                op->d_t2l, op->geom, x_cells, y_cells,
+                                static_cast<cudaStream_t>(stream));
+  });
+}
+
+int sf_diagonal(sf_op* op, int dtype, void* d, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(d, SF_ERR_ARG, "null d");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t es = dsize(dtype);
+    SF_CUDA_CHECK(cudaMemsetAsync(d, 0, op->n_free * es, st));
+    sf::launch_general_diag(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
+                            d, st);
+  });
+}
+
+int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter, int* iters,
+          double* relres, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  int status = guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(b && x, SF_ERR_ARG, "null b or x");
+    SF_REQUIRE(reltol > 0 && maxiter >= 0, SF_ERR_ARG, "bad reltol / maxiter");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double rel = 0.0;
+    int it = 0, outer = 1;
+    if (mode == SF_CG_F64 || mode == SF_CG_F64_PLAIN)
+      it = cg_f64(op, mode == SF_CG_F64, b, x, reltol, maxiter, &rel, st);
+    else if (mode == SF_CG_MIXED)
+      it = cg_mixed(op, b, x, reltol, maxiter, &rel, &outer, st);
+    else
+      throw Error(SF_ERR_ARG, "unknown CG mode");
+    op->last_inner = it;
+    op->last_outer = outer;
+    op->last_relres = rel;
+    if (iters) *iters = it;
+    if (relres) *relres = rel;
+    if (!(rel <= reltol)) throw Error(SF_ERR_NOT_CONVERGED, "CG reached its iteration cap");
+  });
+  return status;
+}
+
+int sf_set_option(sf_op* op, const char* name, double value) {
+  if (!op || !name) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    const std::string n(name);
+    if (n == "mixed_inner_reltol") {
+      SF_REQUIRE(value > 0 && value < 1, SF_ERR_ARG, "mixed_inner_reltol must be in (0,1)");
+      op->mixed_inner_reltol = value;
+    } else if (n == "mixed_max_outer") {
+      SF_REQUIRE(value >= 1, SF_ERR_ARG, "mixed_max_outer must be >= 1");
+      op->mixed_max_outer = (int)value;
+    } else {
+      throw Error(SF_ERR_ARG, "unknown option " + n);
+    }
+  });
+}
+
+int sf_get_info(const sf_op* op, const char* key, double* value) {
+  if (!op || !key || !value) return SF_ERR_ARG;
+  const std::string k(key);
+  const bool tiled = op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64);
+  if (k == "n_free") *value = (double)op->n_free;
+  else if (k == "n_cells") *value = (double)op->cells.ncells;
+  else if (k == "tiled_kernel") *value = tiled ? 1.0 : 0.0;
+  else if (k == "kernels_per_apply") *value = tiled ? (double)sf::cartesian_launches(op->cart) : 1.0;
+  else if (k == "geometry_kind") *value = (double)op->geom.kind;
+  else return SF_ERR_ARG;
+  return SF_OK;
+}
+
+int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres) {
+  if (!op) return SF_ERR_ARG;
+  if (outer) *outer = op->last_outer;
+  if (inner) *inner = op->last_inner;
+  if (relres) *relres = op->last_relres;
+  return SF_OK;
+}
+
+}  // extern "C"

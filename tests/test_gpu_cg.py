@@ -1,0 +1,70 @@
+"""Device CG (FP64 Jacobi, plain, and FP32-inner mixed precision with FP64
+refinement) against the oracle's restatement of IterativeSolvers.cg!."""
+import numpy as np
+import pytest
+
+from oracle import sumfac_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(sf, p, deg, n, perturb=0.0):
+    import torch
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n), perturb=perturb, seed=1)
+    V = sf.FESpace(model, p)
+    m = sf.SumFactorizationMap(3, (p,) * 3, (deg,) * 3)
+    A = sf.LazyMatrix(m, V, V, sf.Measure(model, deg))
+    om = O.make_map(3, p, deg)
+    mesh = O.cartesian_mesh(3, n, p, om, perturb=perturb, seed=1)
+    b = O.rhs(om, mesh, O.sin_forcing)
+    return A, V, om, mesh, b, torch.from_numpy(b).cuda()
+
+
+@pytest.mark.parametrize("mode", ["plain", "jacobi"])
+def test_cg_matches_oracle(sf, mode):
+    A, V, om, mesh, b, bd = setup(sf, 2, 4, 6)
+    S = O.assembled_sparse(om, mesh)
+    pre = None if mode == "plain" else (lambda r, d=S.diagonal(): r / d)
+    x_ref, it_ref, rel_ref = O.cg(lambda v: S @ v, b, reltol=1e-10, precond=pre)
+    x, info = sf.cg(A, bd, reltol=1e-10, mode=mode)
+    assert info["relres"] <= 1e-10 and info["converged"]
+    assert abs(info["iters"] - it_ref) <= 1
+    x = x.cpu().numpy()
+    assert np.abs(x - x_ref).max() < 1e-8 * np.abs(x_ref).max()
+
+
+def test_mixed_precision_reaches_fp64_residual(sf):
+    import torch
+    A, V, om, mesh, b, bd = setup(sf, 4, 8, 4, perturb=0.1)
+    x64, i64 = sf.cg(A, bd, reltol=1e-10, mode="jacobi")
+    xm, im = sf.cg(A, bd, reltol=1e-10, mode="mixed")
+    assert im["relres"] <= 1e-10 and im["outer"] >= 2
+    r = (bd - A @ xm).norm().item() / bd.norm().item()
+    assert r <= 1e-10
+    assert (xm - x64).abs().max().item() < 1e-7 * x64.abs().max().item()
+
+
+def test_discretization_error_decreases(sf):
+    errs = []
+    for n in (2, 4, 8):
+        A, V, om, mesh, b, bd = setup(sf, 2, 6, n)
+        x, info = sf.cg(A, bd, reltol=1e-12, mode="jacobi")
+        X = V.free_dof_coordinates()
+        errs.append(np.abs(x.cpu().numpy() - O.sin_solution(X)).max())
+    assert errs[1] < errs[0] / 6 and errs[2] < errs[1] / 6
+
+
+def test_iteration_cap_is_reported(sf):
+    A, V, om, mesh, b, bd = setup(sf, 2, 4, 6)
+    with pytest.raises(sf.SumFacError) as e:
+        sf.cg(A, bd, reltol=1e-14, maxiter=3)
+    assert e.value.status == 5  # SF_ERR_NOT_CONVERGED
+    x, info = sf.cg(A, bd, reltol=1e-14, maxiter=3, raise_on_fail=False)
+    assert info["iters"] == 3 and not info["converged"]
+
+
+def test_zero_rhs(sf):
+    import torch
+    A, V, om, mesh, b, bd = setup(sf, 2, 4, 3)
+    x, info = sf.cg(A, torch.zeros_like(bd), reltol=1e-10)
+    assert info["iters"] == 0 and x.abs().max().item() == 0.0
