@@ -52,7 +52,14 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    return ap.parse_args()
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--cells", type=int, default=64,
+                    help="cells per direction (64 is the benchmark; smaller only for profiling)")
+    a = ap.parse_args()
+    global NCELL, N_DOF_TOTAL
+    NCELL = a.cells
+    N_DOF_TOTAL = (NCELL * P + 1) ** 3
+    return a
 
 
 # ----------------------------------------------------------------------------
@@ -194,26 +201,29 @@ def run_ours(args, rank, world, local_rank):
     kernel_path = "tiled-cartesian" if A.uses_tiled_kernel() else "general-element"
 
     # end to end through the public host-buffer call (mul! on host vectors)
-    xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
-    yh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
-    xh[:] = x0.cpu().numpy()
-    for _ in range(3):
-        sf.mul(yh, A, xh)
-    ne2e = max(5, min(50, args.steps // 40))
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(ne2e):
-        sf.mul(yh, A, xh)
-    te2e = (time.perf_counter() - t0) / ne2e
-    if world > 1:
-        t = torch.tensor([te2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te2e = t.item()
-    e2e = {"value": round(world * N_DOF_TOTAL / te2e / 1e9, 4), "unit": "GDOF/s",
-           "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8,
-           "ms_per_step": round(te2e * 1e3, 4), "buffers": "pinned host, synchronous sf_mul_host"}
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        yh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        xh[:] = x0.cpu().numpy()
+        for _ in range(3):
+            sf.mul(yh, A, xh)
+        ne2e = max(5, min(50, args.steps // 40))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne2e):
+            sf.mul(yh, A, xh)
+        te2e = (time.perf_counter() - t0) / ne2e
+        if world > 1:
+            t = torch.tensor([te2e], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te2e = t.item()
+        e2e = {"value": round(world * N_DOF_TOTAL / te2e / 1e9, 4), "unit": "GDOF/s",
+               "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8,
+               "ms_per_step": round(te2e * 1e3, 4),
+               "buffers": "pinned host, synchronous sf_mul_host"}
 
     peaks = None
     try:

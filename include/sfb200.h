@@ -41,7 +41,7 @@ typedef struct sf_op sf_op;
 
 /* CG modes for sf_cg */
 #define SF_CG_F64 0           /* FP64 Jacobi-preconditioned CG */
-#define SF_CG_MIXED 1         /* FP32 apply + FP32 inner Jacobi CG, FP64 outer refinement */
+#define SF_CG_MIXED 1         /* FP32 apply + FP32 Jacobi CG recurrence, FP64 reliable updates */
 #define SF_CG_F64_PLAIN 2     /* FP64 CG without a preconditioner (IterativeSolvers default) */
 
 /* Library version (major*10000 + minor*100 + patch). */
@@ -145,16 +145,17 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream);
  * Conjugate gradients on A x = b, device FP64 pointers b and x (x is the
  * initial guess on entry). Replaces IterativeSolvers.cg!(x, A, b) as called
  * at profiling/drivers.jl:85-95. Stops when ||r||_2 <= reltol * ||b||_2
- * (FP64 true residual for SF_CG_MIXED). Reports iterations (total inner
- * iterations for SF_CG_MIXED) and the final relative residual.
+ * (FP64 true residual for SF_CG_MIXED). Reports iterations (FP32 iterations
+ * for SF_CG_MIXED) and the final relative residual.
  */
 int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter,
           int* iters, double* relres, void* stream);
 
 /*
  * Named numeric options of a handle:
- *   "mixed_inner_reltol" : inner FP32 CG relative tolerance of SF_CG_MIXED (default 1e-4)
- *   "mixed_max_outer"    : cap on FP64 refinement steps of SF_CG_MIXED (default 50)
+ *   "mixed_inner_reltol" : SF_CG_MIXED refines (FP64 true residual replaces the FP32
+ *                          recurrence residual) each time the FP32 residual has
+ *                          dropped by this factor (default 0.1)
  */
 int sf_set_option(sf_op* op, const char* name, double value);
 

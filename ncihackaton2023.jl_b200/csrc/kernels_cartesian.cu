@@ -1,22 +1,492 @@
-// Tiled Cartesian kernels. Placeholder until the tiled kernel lands: the
-// structured mesh is served by the general element kernel.
+// Tiled Cartesian kernels: constant-coefficient, axis-aligned affine cells on
+// a structured mesh. This is the fast path of LazyMatrix mul!
+// (src/LazyMatrices.jl:52-61) for the Cartesian meshes that every
+// reference driver builds (profiling/drivers.jl:7-10).
+//
+// Algebra. On such a cell the metric is G(q) = w_q * diag(cx, cy, cz), with w_q
+// the product of 1D weights (the structured_mesh_opt case of the reference's
+// flop model, src/Utils.jl:33-72). Then the element operator
+// sum_r B_r^T G B_r of src/SumFactorizationKernels.jl:40-216 equals, exactly,
+//     cx K(x) M(y) M(z) + cy M(x) K(y) M(z) + cz M(x) M(y) K(z),
+// where M = A0^T W A0 and K = B0^T W B0 are the 1D element matrices with the
+// quadrature already summed. Assembled over a line of cells the structure
+// stays, with M and K assembled along the line:
+//     t1 = M_z x,  t2 = (cz/cy) K_z x,                       (z pass)
+//     a = (cx/cy) M_y t1,  s = K_y t1 + M_y t2,              (y pass)
+//     y = cy (K_x a + M_x s).                                (x pass)
+// This is the same operator up to rounding; the parity tests hold it to 1e-12.
+//
+// Even-odd form. With equispaced nodes in ascending order and a symmetric
+// Gauss rule, M and K are symmetric and centro-symmetric
+// (M[P-i][P-j] = M[i][j]). One cell's 1D product y = M u then splits into an
+// even part (ceil(S/2) square) acting on u_j + u_{P-j} and an odd part
+// (floor(S/2) square) acting on u_j - u_{P-j}, and both parts are symmetric.
+// For P = 4 this takes 21 FP64 operations instead of 25, and 2 x 9 unique
+// constants hold both operators. FP64 FMAs cannot take their operand from the
+// constant bank, so those 18 constants live in registers for the whole kernel.
+//
+// Work decomposition. A CTA owns a box of OUTPUT dofs covering EX x EY x EZ
+// cells: the points (e0 p, (e0+E) p] in each direction. Nothing is scattered,
+// so no atomics and no zeroing of y are needed, and the result is
+// deterministic. The z pass reads x straight from global memory into
+// registers, one z-line per thread, including a one-cell halo in x and y;
+// Dirichlet and out-of-mesh points read as zero. t1/t2 go to shared memory.
+// The y and x passes run one thread per line in shared memory, streaming cell
+// by cell and carrying the vertex shared by neighbouring cells. The output box
+// is written back coalesced.
 #include "sf_cartesian.cuh"
 
+#include <cmath>
+
 namespace sf {
+namespace {
+
+template <int P>
+struct EO {
+  static constexpr int S = P + 1;
+  static constexpr int H = S / 2;           // mirrored pairs (j, P-j)
+  static constexpr bool MID = (S % 2) == 1; // a middle node j = H
+  static constexpr int NE = H + (MID ? 1 : 0);
+  static constexpr int NO = H;
+  static constexpr int UE = NE * (NE + 1) / 2;  // unique entries (upper triangle)
+  static constexpr int UO = NO * (NO + 1) / 2;
+};
+
+__host__ __device__ constexpr int tri(int i, int j, int n) {
+  // packed upper-triangular index of the symmetric pair (i, j), 0 <= i, j < n
+  return i <= j ? i * n - i * (i - 1) / 2 + (j - i) : j * n - j * (j - 1) / 2 + (i - j);
+}
+
+template <int P, typename T>
+struct CartParams {
+  T Me[EO<P>::UE], Mo[EO<P>::UO];  // even / odd parts of M
+  T Ke[EO<P>::UE], Ko[EO<P>::UO];  // even / odd parts of K
+  T rz, rx, cy;                    // cz/cy, cx/cy, cy
+  const T* x;
+  T* y;
+  int nfx, nfy, nfz;  // free grid
+  int ntx, nty, ntz;  // tiles
+};
+
+// Even/odd parts of one operator, held in registers (symmetric entries share one register).
+template <int P, typename T>
+struct EOMat {
+  using S = EO<P>;
+  T e[S::NE][S::NE];
+  T o[S::NO > 0 ? S::NO : 1][S::NO > 0 ? S::NO : 1];
+  __device__ __forceinline__ void load(const T* ue, const T* uo) {
+#pragma unroll
+    for (int i = 0; i < S::NE; ++i)
+#pragma unroll
+      for (int j = i; j < S::NE; ++j) {
+        const T v = ue[tri(i, j, S::NE)];
+        e[i][j] = v;
+        e[j][i] = v;
+      }
+#pragma unroll
+    for (int i = 0; i < S::NO; ++i)
+#pragma unroll
+      for (int j = i; j < S::NO; ++j) {
+        const T v = uo[tri(i, j, S::NO)];
+        o[i][j] = v;
+        o[j][i] = v;
+      }
+  }
+};
+
+template <int P, typename T>
+struct Split {  // u_j + u_{P-j} (and the middle node) / u_j - u_{P-j}
+  T e[EO<P>::NE];
+  T o[EO<P>::NO > 0 ? EO<P>::NO : 1];
+};
+
+template <int P, typename T>
+__device__ __forceinline__ Split<P, T> split(const T (&u)[P + 1]) {
+  using S = EO<P>;
+  Split<P, T> s;
+#pragma unroll
+  for (int j = 0; j < S::H; ++j) {
+    s.e[j] = u[j] + u[P - j];
+    s.o[j] = u[j] - u[P - j];
+  }
+  if constexpr (S::MID) s.e[S::H] = u[S::H];
+  return s;
+}
+
+// (ye, yo) += (E e, O o)
+template <int P, typename T>
+__device__ __forceinline__ void mac(const EOMat<P, T>& A, const Split<P, T>& s, T (&ye)[EO<P>::NE],
+                                   T (&yo)[EO<P>::NO > 0 ? EO<P>::NO : 1]) {
+  using S = EO<P>;
+#pragma unroll
+  for (int i = 0; i < S::NE; ++i)
+#pragma unroll
+    for (int j = 0; j < S::NE; ++j) ye[i] = fma(A.e[i][j], s.e[j], ye[i]);
+#pragma unroll
+  for (int i = 0; i < S::NO; ++i)
+#pragma unroll
+    for (int j = 0; j < S::NO; ++j) yo[i] = fma(A.o[i][j], s.o[j], yo[i]);
+}
+
+// row 0 only: E[0] . e + O[0] . o
+template <int P, typename T>
+__device__ __forceinline__ T mac_row0(const EOMat<P, T>& A, const Split<P, T>& s, T acc) {
+  using S = EO<P>;
+#pragma unroll
+  for (int j = 0; j < S::NE; ++j) acc = fma(A.e[0][j], s.e[j], acc);
+#pragma unroll
+  for (int j = 0; j < S::NO; ++j) acc = fma(A.o[0][j], s.o[j], acc);
+  return acc;
+}
+
+template <int P, typename T>
+struct Acc {  // even/odd accumulators of one output line
+  T e[EO<P>::NE];
+  T o[EO<P>::NO > 0 ? EO<P>::NO : 1];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int i = 0; i < EO<P>::NE; ++i) e[i] = T(0);
+#pragma unroll
+    for (int i = 0; i < EO<P>::NO; ++i) o[i] = T(0);
+  }
+  // value at local node l
+  __device__ __forceinline__ T at(int l) const {
+    using S = EO<P>;
+    if (S::MID && l == S::H) return e[S::H];
+    if (l < S::H) return e[l] + o[l];
+    return e[P - l] - o[P - l];
+  }
+};
+
+template <int P, int EX, int EY, int EZ>
+struct Tile {
+  static constexpr int BX = (EX + 1) * P + 1, BY = (EY + 1) * P + 1, BZ = (EZ + 1) * P + 1;
+  static constexpr int OX = EX * P, OY = EY * P, OZ = EZ * P;
+  static constexpr int PLANE = BX * BY;
+  static constexpr int TS = PLANE * OZ;  // each of t1 (-> a -> y) and t2 (-> s)
+  static constexpr int WORDS = 2 * TS;
+};
+
+// Generic streaming pass over a line of E+1 cells held in shared memory.
+// NIN input lines (stride `st`), NOUT output lines written in place over the
+// inputs at index (o-1)*st for the owned points o = 1..E*P. `body` forms the
+// even/odd accumulators of every output from the split inputs; `row0` forms
+// only the node-0 values (last cell).
+template <int P, int E, int NIN, int NOUT, typename T, typename Body, typename Row0, typename Fin>
+__device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body& body,
+                                          const Row0& row0, const Fin& fin) {
+  T u[NIN][P + 1];
+  T carry[NOUT];
+#pragma unroll
+  for (int j = 0; j < NOUT; ++j) carry[j] = T(0);
+#pragma unroll 1
+  for (int k = 0; k < E; ++k) {
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) {
+#pragma unroll
+      for (int l = 0; l <= P; ++l)
+        if (k == 0 || l > 0) u[i][l] = ln[i][(k * P + l) * st];
+    }
+    Split<P, T> s[NIN];
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) s[i] = split<P, T>(u[i]);
+    Acc<P, T> acc[NOUT];
+#pragma unroll
+    for (int j = 0; j < NOUT; ++j) acc[j].zero();
+    body(s, acc);
+#pragma unroll
+    for (int j = 0; j < NOUT; ++j) {
+      if (k > 0) ln[j][(k * P - 1) * st] = fin(j, acc[j].at(0) + carry[j]);
+#pragma unroll
+      for (int l = 1; l < P; ++l) ln[j][(k * P + l - 1) * st] = fin(j, acc[j].at(l));
+      carry[j] = acc[j].at(P);
+    }
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) u[i][0] = u[i][P];
+  }
+  // last cell: node 0 only (the end point E*P)
+#pragma unroll
+  for (int i = 0; i < NIN; ++i)
+#pragma unroll
+    for (int l = 1; l <= P; ++l) u[i][l] = ln[i][(E * P + l) * st];
+  Split<P, T> s[NIN];
+#pragma unroll
+  for (int i = 0; i < NIN; ++i) s[i] = split<P, T>(u[i]);
+  T r[NOUT];
+  row0(s, r);
+#pragma unroll
+  for (int j = 0; j < NOUT; ++j) ln[j][(E * P - 1) * st] = fin(j, r[j] + carry[j]);
+}
+
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
+  using G = Tile<P, EX, EY, EZ>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* T1 = reinterpret_cast<T*>(smem_raw);  // t1 -> a -> y   [OZ][BY][BX]
+  T* T2 = T1 + G::TS;                        // t2 -> s        [OZ][BY][BX]
+
+  EOMat<P, T> Mm, Km;
+  Mm.load(Q.Me, Q.Mo);
+  Km.load(Q.Ke, Q.Ko);
+
+  const int tile = blockIdx.x;
+  const int tx = tile % Q.ntx;
+  const int ty = (tile / Q.ntx) % Q.nty;
+  const int tz = tile / (Q.ntx * Q.nty);
+  // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
+  const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
+  const int nfx = Q.nfx, nfy = Q.nfy, nfz = Q.nfz;
+  const long long pz = (long long)nfx * nfy;
+
+  // ---- z pass: one z-line per thread, read from global memory ----
+  for (int l = threadIdx.x; l < G::PLANE; l += NT) {
+    const int x = l % G::BX, y = l / G::BX;
+    const int fx = fx0 + x, fy = fy0 + y;
+    const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
+    const T* col = Q.x + (long long)fx + (long long)nfx * fy;
+    T c[G::BZ];
+#pragma unroll
+    for (int z = 0; z < G::BZ; ++z) {
+      const int fz = fz0 + z;
+      c[z] = (inxy && (unsigned)fz < (unsigned)nfz) ? col[fz * pz] : T(0);
+    }
+    T cm = T(0), ck = T(0);
+#pragma unroll
+    for (int k = 0; k < EZ; ++k) {
+      T u[P + 1];
+#pragma unroll
+      for (int m = 0; m <= P; ++m) u[m] = c[k * P + m];
+      const Split<P, T> s = split<P, T>(u);
+      Acc<P, T> am, ak;
+      am.zero();
+      ak.zero();
+      mac<P, T>(Mm, s, am.e, am.o);
+      mac<P, T>(Km, s, ak.e, ak.o);
+      if (k > 0) {
+        T1[(k * P - 1) * G::PLANE + l] = am.at(0) + cm;
+        const T v = ak.at(0) + ck;
+        T2[(k * P - 1) * G::PLANE + l] = ISO ? v : v * Q.rz;
+      }
+#pragma unroll
+      for (int m = 1; m < P; ++m) {
+        T1[(k * P + m - 1) * G::PLANE + l] = am.at(m);
+        const T v = ak.at(m);
+        T2[(k * P + m - 1) * G::PLANE + l] = ISO ? v : v * Q.rz;
+      }
+      cm = am.at(P);
+      ck = ak.at(P);
+    }
+    {
+      T u[P + 1];
+#pragma unroll
+      for (int m = 0; m <= P; ++m) u[m] = c[EZ * P + m];
+      const Split<P, T> s = split<P, T>(u);
+      T1[(EZ * P - 1) * G::PLANE + l] = mac_row0<P, T>(Mm, s, cm);
+      const T v = mac_row0<P, T>(Km, s, ck);
+      T2[(EZ * P - 1) * G::PLANE + l] = ISO ? v : v * Q.rz;
+    }
+  }
+  __syncthreads();
+
+  // ---- y pass: lines (x, zo): a = rx M t1 -> T1, s = K t1 + M t2 -> T2 ----
+  for (int l = threadIdx.x; l < G::BX * G::OZ; l += NT) {
+    const int x = l % G::BX, zo = l / G::BX;
+    T* const ln[2] = {T1 + zo * G::PLANE + x, T2 + zo * G::PLANE + x};
+    smem_line<P, EY, 2, 2, T>(
+        ln, G::BX,
+        [&](const Split<P, T>(&s)[2], Acc<P, T>(&acc)[2]) {
+          mac<P, T>(Mm, s[0], acc[0].e, acc[0].o);
+          mac<P, T>(Km, s[0], acc[1].e, acc[1].o);
+          mac<P, T>(Mm, s[1], acc[1].e, acc[1].o);
+        },
+        [&](const Split<P, T>(&s)[2], T(&r)[2]) {
+          r[0] = mac_row0<P, T>(Mm, s[0], T(0));
+          r[1] = mac_row0<P, T>(Mm, s[1], mac_row0<P, T>(Km, s[0], T(0)));
+        },
+        [&](int j, T v) { return (ISO || j == 1) ? v : v * Q.rx; });
+  }
+  __syncthreads();
+
+  // ---- x pass: lines (yo, zo): y = cy (K a + M s) -> T1 ----
+  for (int l = threadIdx.x; l < G::OY * G::OZ; l += NT) {
+    const int yo = l % G::OY, zo = l / G::OY;
+    T* const ln[2] = {T1 + zo * G::PLANE + yo * G::BX, T2 + zo * G::PLANE + yo * G::BX};
+    smem_line<P, EX, 2, 1, T>(
+        ln, 1,
+        [&](const Split<P, T>(&s)[2], Acc<P, T>(&acc)[1]) {
+          mac<P, T>(Km, s[0], acc[0].e, acc[0].o);
+          mac<P, T>(Mm, s[1], acc[0].e, acc[0].o);
+        },
+        [&](const Split<P, T>(&s)[2], T(&r)[1]) {
+          r[0] = mac_row0<P, T>(Mm, s[1], mac_row0<P, T>(Km, s[0], T(0)));
+        },
+        [&](int, T v) { return v * Q.cy; });
+  }
+  __syncthreads();
+
+  // ---- store the owned outputs (free coords start at e0*p) ----
+  const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
+  for (int i = threadIdx.x; i < G::OX * G::OY * G::OZ; i += NT) {
+    const int xo = i % G::OX;
+    const int r = i / G::OX;
+    const int yo = r % G::OY;
+    const int zo = r / G::OY;
+    const int fx = ox0 + xo, fy = oy0 + yo, fz = oz0 + zo;
+    if (fx < nfx && fy < nfy && fz < nfz)
+      Q.y[(long long)fx + (long long)nfx * (fy + (long long)nfy * fz)] =
+          T1[zo * G::PLANE + yo * G::BX + xo];
+  }
+}
+
+// Tile shapes per (P, dtype). Shared memory is 2 * (E*P+P+1)^2 * EZ*P words.
+template <int P, typename T>
+struct Config;
+#define SF_CART_CONFIG(P_, T_, EX_, EY_, EZ_, NT_, MINB_)                   \
+  template <>                                                               \
+  struct Config<P_, T_> {                                                   \
+    static constexpr int EX = EX_, EY = EY_, EZ = EZ_, NT = NT_, MINB = MINB_; \
+  };
+SF_CART_CONFIG(1, double, 8, 8, 4, 256, 2)
+SF_CART_CONFIG(2, double, 4, 4, 4, 256, 2)
+SF_CART_CONFIG(3, double, 4, 4, 2, 256, 2)
+SF_CART_CONFIG(4, double, 4, 4, 2, 256, 3)
+SF_CART_CONFIG(5, double, 2, 2, 2, 256, 2)
+SF_CART_CONFIG(6, double, 2, 2, 2, 256, 1)
+SF_CART_CONFIG(7, double, 2, 2, 1, 256, 1)
+SF_CART_CONFIG(8, double, 2, 2, 1, 256, 1)
+SF_CART_CONFIG(1, float, 8, 8, 4, 256, 2)
+SF_CART_CONFIG(2, float, 4, 4, 4, 256, 2)
+SF_CART_CONFIG(3, float, 4, 4, 4, 256, 2)
+SF_CART_CONFIG(4, float, 4, 4, 2, 256, 3)
+SF_CART_CONFIG(5, float, 2, 2, 2, 256, 2)
+SF_CART_CONFIG(6, float, 2, 2, 2, 256, 2)
+SF_CART_CONFIG(7, float, 2, 2, 2, 256, 2)
+SF_CART_CONFIG(8, float, 2, 2, 1, 256, 2)
+#undef SF_CART_CONFIG
+
+template <int P, typename T>
+void fill_eo(const double* M, double scale, T* ue, T* uo) {
+  using S = EO<P>;
+  auto m = [&](int i, int j) { return scale * M[i * (P + 1) + j]; };
+  for (int i = 0; i < S::NE; ++i)
+    for (int j = i; j < S::NE; ++j) {
+      double v;
+      if (i < S::H && j < S::H) v = 0.5 * (m(i, j) + m(i, P - j));
+      else v = m(i, j);  // a middle row or column
+      ue[tri(i, j, S::NE)] = (T)v;
+    }
+  for (int i = 0; i < S::NO; ++i)
+    for (int j = i; j < S::NO; ++j) uo[tri(i, j, S::NO)] = (T)(0.5 * (m(i, j) - m(i, P - j)));
+}
+
+template <int P, typename T>
+void run_cartesian(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st) {
+  using C = Config<P, T>;
+  using G = Tile<P, C::EX, C::EY, C::EZ>;
+  CartParams<P, T> Q{};
+  fill_eo<P, T>(plan.M, 1.0, Q.Me, Q.Mo);
+  fill_eo<P, T>(plan.K, 1.0, Q.Ke, Q.Ko);
+  const double cx = plan.c[0], cy = plan.c[1], cz = plan.c[2];
+  Q.rz = (T)(cz / cy);
+  Q.rx = (T)(cx / cy);
+  Q.cy = (T)cy;
+  const bool iso = (cx == cy) && (cz == cy);
+  Q.x = static_cast<const T*>(x);
+  Q.y = static_cast<T*>(y);
+  Q.nfx = plan.nx * P - 1;
+  Q.nfy = plan.ny * P - 1;
+  Q.nfz = plan.nz * P - 1;
+  Q.ntx = (plan.nx + C::EX - 1) / C::EX;
+  Q.nty = (plan.ny + C::EY - 1) / C::EY;
+  Q.ntz = (plan.nz + C::EZ - 1) / C::EZ;
+  const long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
+  SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
+  const size_t smem = (size_t)G::WORDS * sizeof(T);
+  if (iso) {
+    auto kern = k_cartesian<P, C::EX, C::EY, C::EZ, C::NT, true, T, C::MINB>;
+    SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)tiles, C::NT, smem, st>>>(Q);
+  } else {
+    auto kern = k_cartesian<P, C::EX, C::EY, C::EZ, C::NT, false, T, C::MINB>;
+    SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(unsigned)tiles, C::NT, smem, st>>>(Q);
+  }
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void dispatch(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st) {
+  switch (plan.SB - 1) {
+    case 1: return run_cartesian<1, T>(plan, x, y, st);
+    case 2: return run_cartesian<2, T>(plan, x, y, st);
+    case 3: return run_cartesian<3, T>(plan, x, y, st);
+    case 4: return run_cartesian<4, T>(plan, x, y, st);
+    case 5: return run_cartesian<5, T>(plan, x, y, st);
+    case 6: return run_cartesian<6, T>(plan, x, y, st);
+    case 7: return run_cartesian<7, T>(plan, x, y, st);
+    case 8: return run_cartesian<8, T>(plan, x, y, st);
+    default: throw Error(SF_ERR_UNSUPPORTED, "no tiled Cartesian kernel for this order");
+  }
+}
+
+}  // namespace
 
 bool cartesian_prepare(CartesianPlan& plan, int SB, int SQ, const double* A, const double* B,
                        const double* w1, const double* G0, int nx, int ny, int nz) {
   plan.ready = false;
-  return false;
+  if (SB < 2 || SB > 9) return false;
+  if (!(G0[0] > 0 && G0[1] > 0 && G0[2] > 0)) return false;
+  plan.SB = SB;
+  plan.SQ = SQ;
+  plan.nx = nx;
+  plan.ny = ny;
+  plan.nz = nz;
+  // M = A^T W A, K = B^T W B (1D, kernel order = lexicographic along the segment)
+  double mmax = 0.0, kmax = 0.0;
+  for (int l = 0; l < SB; ++l)
+    for (int m = 0; m < SB; ++m) {
+      double mm = 0.0, kk = 0.0;
+      for (int q = 0; q < SQ; ++q) {
+        mm += w1[q] * A[q * SB + l] * A[q * SB + m];
+        kk += w1[q] * B[q * SB + l] * B[q * SB + m];
+      }
+      plan.M[l * SB + m] = mm;
+      plan.K[l * SB + m] = kk;
+      mmax = std::fmax(mmax, std::fabs(mm));
+      kmax = std::fmax(kmax, std::fabs(kk));
+    }
+  // the even-odd form needs symmetric, centro-symmetric M and K
+  const int P = SB - 1;
+  for (int l = 0; l < SB; ++l)
+    for (int m = 0; m < SB; ++m) {
+      const double* Ms = plan.M;
+      const double* Ks = plan.K;
+      if (std::fabs(Ms[l * SB + m] - Ms[m * SB + l]) > 1e-13 * mmax ||
+          std::fabs(Ms[l * SB + m] - Ms[(P - l) * SB + (P - m)]) > 1e-13 * mmax ||
+          std::fabs(Ks[l * SB + m] - Ks[m * SB + l]) > 1e-13 * kmax ||
+          std::fabs(Ks[l * SB + m] - Ks[(P - l) * SB + (P - m)]) > 1e-13 * kmax)
+        return false;
+    }
+  plan.c[0] = G0[0];
+  plan.c[1] = G0[1];
+  plan.c[2] = G0[2];
+  plan.ready = true;
+  return true;
 }
 
-bool cartesian_supported(const CartesianPlan& plan, int dtype) { return false; }
+bool cartesian_supported(const CartesianPlan& plan, int dtype) {
+  return plan.ready && (dtype == SF_F64 || dtype == SF_F32) && plan.SB >= 2 && plan.SB <= 9;
+}
 
 int cartesian_launches(const CartesianPlan& plan) { return 1; }
 
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
                      cudaStream_t stream) {
-  throw Error(SF_ERR_UNSUPPORTED, "tiled Cartesian kernel not available");
+  SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
+  if (dtype == SF_F64) dispatch<double>(plan, x, y, stream);
+  else if (dtype == SF_F32) dispatch<float>(plan, x, y, stream);
+  else throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
 }
 
 void cartesian_release(CartesianPlan& plan) { plan.ready = false; }

@@ -138,39 +138,38 @@ __global__ void k_invert(const double* __restrict__ d, T* __restrict__ dinv, lon
     dinv[i] = (T)(1.0 / d[i]);
 }
 
-// Mixed precision: r64 = b - q64, sums (r,r); r32 = r64 * scale where scale = 1/||r|| is
-// applied in a second pass (k_scale_to_f32) once ||r|| is known.
-__global__ void k_residual64(const double* __restrict__ b, const double* __restrict__ q,
-                             double* __restrict__ r, long long n, double* __restrict__ partials) {
-  double v[1] = {0.0};
+// Reliable update of the mixed-precision CG: the FP64 true residual
+// r = b - A64 x replaces the FP32 recurrence residual. Writes r32 = (float) r,
+// zeroes the FP32 partial solution xs32, and (when set_p) starts the search
+// direction p32 = dinv r32. Sums: (r32, dinv r32) and the FP64 (r, r).
+__global__ void k_mixed_residual(const double* __restrict__ b, const double* __restrict__ q,
+                                 const float* __restrict__ dinv, float* __restrict__ r32,
+                                 float* __restrict__ xs32, float* __restrict__ p32, int set_p,
+                                 long long n, double* __restrict__ partials) {
+  double v[2] = {0.0, 0.0};
   for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kThreads) {
     const double ri = b[i] - q[i];
-    r[i] = ri;
-    v[0] += ri * ri;
+    const float rf = (float)ri;
+    const float zf = dinv[i] * rf;
+    r32[i] = rf;
+    xs32[i] = 0.0f;
+    if (set_p) p32[i] = zf;
+    v[0] += (double)rf * (double)zf;
+    v[1] += ri * ri;
   }
-  block_sum<1>(v);
-  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
-}
-
-__global__ void k_scale_to_f32(const double* __restrict__ s, int slot, const double* __restrict__ r,
-                               float* __restrict__ r32, float* __restrict__ d32, long long n) {
-  const double nr = sqrt(s[slot]);
-  const double scale = nr > 0.0 ? 1.0 / nr : 0.0;
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    r32[i] = (float)(r[i] * scale);
-    d32[i] = 0.0f;
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x * 2 + 0] = v[0];
+    partials[blockIdx.x * 2 + 1] = v[1];
   }
 }
 
-// x64 += ||r|| * d32
-__global__ void k_correct(const double* __restrict__ s, int slot, double* __restrict__ x,
-                          const float* __restrict__ d32, long long n) {
-  const double nr = sqrt(s[slot]);
+// x64 += xs32 (fold the FP32 partial solution into the FP64 solution)
+__global__ void k_fold(double* __restrict__ x, const float* __restrict__ xs32, long long n) {
   for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kThreads)
-    x[i] = fma(nr, (double)d32[i], x[i]);
+    x[i] += (double)xs32[i];
 }
 
 int grid_for(long long n) {
@@ -224,23 +223,22 @@ void vec_invert(const double* d, T* dinv, long long n, cudaStream_t st) {
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-void mixed_residual(const double* b, const double* q, double* r, long long n, double* partials,
-                    double* s, int slot, cudaStream_t st) {
+void mixed_residual(const double* b, const double* q, const float* dinv, float* r32, float* xs32,
+                    float* p32, bool set_p, long long n, double* partials, double* s,
+                    cudaStream_t st) {
   const int g = grid_for(n);
-  k_residual64<<<g, kThreads, 0, st>>>(b, q, r, n, partials);
-  k_finish<1><<<1, kThreads, 0, st>>>(partials, g, s + slot);
+  k_mixed_residual<<<g, kThreads, 0, st>>>(b, q, dinv, r32, xs32, p32, set_p ? 1 : 0, n, partials);
+  k_finish<2><<<1, kThreads, 0, st>>>(partials, g, s + CG_RZ_NEW);  // RZ_NEW, RR (FP64 true)
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-void mixed_scale(const double* s, int slot, const double* r, float* r32, float* d32, long long n,
-                 cudaStream_t st) {
-  k_scale_to_f32<<<grid_for(n), kThreads, 0, st>>>(s, slot, r, r32, d32, n);
+void mixed_fold(double* x, const float* xs32, long long n, cudaStream_t st) {
+  k_fold<<<grid_for(n), kThreads, 0, st>>>(x, xs32, n);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-void mixed_correct(const double* s, int slot, double* x, const float* d32, long long n,
-                   cudaStream_t st) {
-  k_correct<<<grid_for(n), kThreads, 0, st>>>(s, slot, x, d32, n);
+void copy_scalar(double* s, int dst, int src, cudaStream_t st) {
+  k_copy_scalar<<<1, 32, 0, st>>>(s, dst, src);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 

@@ -12,7 +12,6 @@ enum CgSlot {
   CG_RZ_NEW = 2,  // (r, z) after the update; CG_RR must follow it
   CG_RR = 3,      // (r, r)
   CG_BB = 4,      // (b, b); must follow CG_RR
-  CG_RES64 = 5,   // mixed precision: FP64 outer residual (r, r)
   CG_NSLOTS = 8
 };
 
@@ -30,11 +29,13 @@ template <typename T>
 void cg_direction(double* s, T* p, const T* r, const T* dinv, long long n, cudaStream_t st);
 template <typename T>
 void vec_invert(const double* d, T* dinv, long long n, cudaStream_t st);
-void mixed_residual(const double* b, const double* q, double* r, long long n, double* partials,
-                    double* s, int slot, cudaStream_t st);
-void mixed_scale(const double* s, int slot, const double* r, float* r32, float* d32, long long n,
-                 cudaStream_t st);
-void mixed_correct(const double* s, int slot, double* x, const float* d32, long long n,
-                   cudaStream_t st);
+// Reliable update: r32 = float(b - q), xs32 = 0, optionally p32 = dinv r32;
+// writes s[CG_RZ_NEW] = (r32, dinv r32) and s[CG_RR] = FP64 (r, r).
+void mixed_residual(const double* b, const double* q, const float* dinv, float* r32, float* xs32,
+                    float* p32, bool set_p, long long n, double* partials, double* s,
+                    cudaStream_t st);
+// x += xs32
+void mixed_fold(double* x, const float* xs32, long long n, cudaStream_t st);
+void copy_scalar(double* s, int dst, int src, cudaStream_t st);
 
 }  // namespace sf

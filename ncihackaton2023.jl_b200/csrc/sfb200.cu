@@ -42,8 +42,7 @@ struct sf_op {
   double* d_hx = nullptr;    // sf_mul_host staging
   double* d_hy = nullptr;
   double* h_scalar = nullptr;  // pinned
-  double mixed_inner_reltol = 1e-4;
-  int mixed_max_outer = 50;
+  double mixed_inner_reltol = 1e-1;
   int last_outer = 0, last_inner = 0;
   double last_relres = 0.0;
   std::string err;
@@ -231,7 +230,13 @@ int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, in
   return it;
 }
 
-// FP32 apply + FP32 inner Jacobi CG with FP64 dots; FP64 outer refinement.
+// Mixed-precision Jacobi CG with reliable updates. The CG recurrence (p, q,
+// r, the partial solution xs) runs in FP32 with the FP32 apply; dot products
+// accumulate in FP64. Whenever the FP32 residual has dropped by the factor
+// `mixed_inner_reltol` since the last update (or below the target), the
+// partial solution is folded into the FP64 solution x, and the FP64 true
+// residual b - A64 x replaces r. The search direction is kept, so the Krylov
+// recurrence is not restarted. The stopping test uses the FP64 true residual only.
 int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, double* relres,
              int* outer_out, cudaStream_t st) {
   const long long n = op->n_free;
@@ -239,57 +244,58 @@ int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, 
   const size_t v4 = align256(n * sizeof(float));
   const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
   const size_t pb = align256(sf::kRedBlocks * 3 * sizeof(double));
-  char* ws = static_cast<char*>(workspace(op, 2 * v8 + 6 * v4 + sb + pb));
-  double* r64 = reinterpret_cast<double*>(ws);
-  double* q64 = reinterpret_cast<double*>(ws + v8);
-  char* w4 = ws + 2 * v8;
-  float* rhs32 = reinterpret_cast<float*>(w4);
-  float* d32 = reinterpret_cast<float*>(w4 + v4);
-  float* r32 = reinterpret_cast<float*>(w4 + 2 * v4);
-  float* p32 = reinterpret_cast<float*>(w4 + 3 * v4);
-  float* q32 = reinterpret_cast<float*>(w4 + 4 * v4);
-  float* dinv32 = reinterpret_cast<float*>(w4 + 5 * v4);
-  double* s = reinterpret_cast<double*>(ws + 2 * v8 + 6 * v4);
-  double* partials = reinterpret_cast<double*>(ws + 2 * v8 + 6 * v4 + sb);
+  char* ws = static_cast<char*>(workspace(op, v8 + 5 * v4 + sb + pb));
+  double* q64 = reinterpret_cast<double*>(ws);
+  char* w4 = ws + v8;
+  float* xs32 = reinterpret_cast<float*>(w4);
+  float* r32 = reinterpret_cast<float*>(w4 + v4);
+  float* p32 = reinterpret_cast<float*>(w4 + 2 * v4);
+  float* q32 = reinterpret_cast<float*>(w4 + 3 * v4);
+  float* dinv32 = reinterpret_cast<float*>(w4 + 4 * v4);
+  double* s = reinterpret_cast<double*>(ws + v8 + 5 * v4);
+  double* partials = reinterpret_cast<double*>(ws + v8 + 5 * v4 + sb);
   ensure_diag(op, st);
   sf::vec_invert<float>(op->d_diag, dinv32, n, st);
-  // ||b||
   sf::vec_dot<double>(b, b, n, partials, s + sf::CG_BB, st);
   const double bb = read_scalar(op, s, sf::CG_BB, st);
   const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
   const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
-  const double eta2 = op->mixed_inner_reltol * op->mixed_inner_reltol;
-  int inner_total = 0, outer = 0;
-  double rr64 = 0.0;
-  for (;;) {
-    apply_impl(op, SF_F64, x, q64, st);
-    sf::mixed_residual(b, q64, r64, n, partials, s, sf::CG_RES64, st);
-    rr64 = read_scalar(op, s, sf::CG_RES64, st);
-    SF_REQUIRE(std::isfinite(rr64), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
-    if (rr64 <= tol2 || inner_total >= maxiter || outer >= op->mixed_max_outer) break;
-    ++outer;
-    sf::mixed_scale(s, sf::CG_RES64, r64, rhs32, d32, n, st);
-    // inner CG from d = 0 on A d = rhs32 (||rhs32|| = 1)
-    sf::cg_start<float>(rhs32, nullptr, dinv32, r32, p32, n, partials, s, st);
-    double rr = read_scalar(op, s, sf::CG_RR, st);
-    const double itol2 = eta2 * rr;
-    int it = 0;
-    while (rr > itol2 && inner_total < maxiter) {
-      apply_impl(op, SF_F32, p32, q32, st);
-      sf::vec_dot<float>(p32, q32, n, partials, s + sf::CG_PQ, st);
-      sf::cg_update<float>(s, d32, p32, r32, q32, dinv32, n, partials, s, st);
-      rr = read_scalar(op, s, sf::CG_RR, st);
-      ++it;
-      ++inner_total;
-      SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in inner CG");
-      if (rr <= itol2) break;
-      sf::cg_direction<float>(s, p32, r32, dinv32, n, st);
+  const double delta2 = op->mixed_inner_reltol * op->mixed_inner_reltol;
+  // true residual of the initial guess; p = dinv r
+  apply_impl(op, SF_F64, x, q64, st);
+  sf::mixed_residual(b, q64, dinv32, r32, xs32, p32, true, n, partials, s, st);
+  sf::copy_scalar(s, sf::CG_RZ, sf::CG_RZ_NEW, st);
+  double rr64 = read_scalar(op, s, sf::CG_RR, st);
+  SF_REQUIRE(std::isfinite(rr64), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
+  double rr_ref = rr64;
+  int it = 0, updates = 0;
+  bool dirty = false;  // xs32 holds a partial solution not yet folded into x
+  while (rr64 > tol2 && it < maxiter) {
+    apply_impl(op, SF_F32, p32, q32, st);
+    sf::vec_dot<float>(p32, q32, n, partials, s + sf::CG_PQ, st);
+    sf::cg_update<float>(s, xs32, p32, r32, q32, dinv32, n, partials, s, st);
+    const double rr = read_scalar(op, s, sf::CG_RR, st);
+    ++it;
+    dirty = true;
+    SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
+    if (rr <= delta2 * rr_ref || rr <= tol2 || it >= maxiter) {
+      // reliable update: fold xs into x, replace r by the FP64 true residual
+      sf::mixed_fold(x, xs32, n, st);
+      apply_impl(op, SF_F64, x, q64, st);
+      sf::mixed_residual(b, q64, dinv32, r32, xs32, p32, false, n, partials, s, st);
+      rr64 = read_scalar(op, s, sf::CG_RR, st);
+      SF_REQUIRE(std::isfinite(rr64), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
+      rr_ref = rr64;
+      dirty = false;
+      ++updates;
+      if (rr64 <= tol2) break;
     }
-    sf::mixed_correct(s, sf::CG_RES64, x, d32, n, st);
+    sf::cg_direction<float>(s, p32, r32, dinv32, n, st);
   }
+  if (dirty) sf::mixed_fold(x, xs32, n, st);
   *relres = std::sqrt(rr64) / nb;
-  *outer_out = outer;
-  return inner_total;
+  *outer_out = updates;
+  return it;
 }
 
 }  // namespace
@@ -652,9 +658,6 @@ int sf_set_option(sf_op* op, const char* name, double value) {
     if (n == "mixed_inner_reltol") {
       SF_REQUIRE(value > 0 && value < 1, SF_ERR_ARG, "mixed_inner_reltol must be in (0,1)");
       op->mixed_inner_reltol = value;
-    } else if (n == "mixed_max_outer") {
-      SF_REQUIRE(value >= 1, SF_ERR_ARG, "mixed_max_outer must be >= 1");
-      op->mixed_max_outer = (int)value;
     } else {
       throw Error(SF_ERR_ARG, "unknown option " + n);
     }
