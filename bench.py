@@ -42,6 +42,9 @@ P, DEG, NCELL = 4, 8, 64
 N_DOF_TOTAL = (NCELL * P + 1) ** 3  # 16,974,593
 METRIC = "Q4 64^3 Laplacian apply GDOF/s; CG time to relres 1e-10, mixed vs FP64, 1 B200"
 WORKLOAD = "Q4 64^3 affine hex, 5-pt Gauss, homogeneous Dirichlet, FP64 apply y=Ax"
+# DRAM bytes (read + write) of one apply launch on this workload, from one ncu
+# capture of the kernel (dram__bytes_read.sum + dram__bytes_write.sum).
+NCU_TRAFFIC_BYTES = {"tiled-cartesian": 224.4e6}
 
 
 def parse():
@@ -243,7 +246,8 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": e2e,
         "gpu_launches": args.steps * A.kernels_per_apply(),
-        "roofline": roofline_entry(achieved, peaks, None),
+        "roofline": roofline_entry(achieved, peaks,
+                                   NCU_TRAFFIC_BYTES.get(kernel_path) if NCELL == 64 else None),
         "flops_reference_model": {"per_apply_gflop": 5.996544, "achieved_tflops":
                                   round(5.996544 / (ms_step * 1e-3) / 1e3, 3)},
     }
