@@ -171,6 +171,29 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  */
 int sf_get_info(const sf_op* op, const char* key, double* value);
 
+/*
+ * sf_cg_noalloc: sf_cg without any device or pinned-host allocation. It has no
+ * counterpart in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc: for example, a host whose
+ * device memory is owned by its own pool allocator (CUDA.jl's and PyTorch's
+ * caching allocators keep freed memory for reuse), or a time-critical loop
+ * that cannot afford the device-wide synchronisation that cudaMalloc/cudaFree
+ * can cause. Same arguments and stopping rule as sf_cg. Modes SF_CG_F64 and
+ * SF_CG_F64_PLAIN only (SF_CG_MIXED returns SF_ERR_UNSUPPORTED).
+ *
+ * Limits and sharing:
+ * - Its scratch is one static device array sized for n_free <= SF_NOALLOC_MAX_FREE
+ *   (about 10 MB). Every GPU that loads the library holds it until exit.
+ *   Larger problems are rejected with SF_ERR_ARG.
+ * - The first call on each device looks up the array's device address. Make
+ *   that first call before any stream capture.
+ * - All calls share the array: calls that overlap on the GPU race.
+ */
+#define SF_NOALLOC_MAX_FREE 262144
+int sf_cg_noalloc(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter,
+                  int* iters, double* relres, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

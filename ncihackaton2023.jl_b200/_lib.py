@@ -61,7 +61,10 @@ SIGNATURES = {
     "sf_set_option": (i32, [vp, C.c_char_p, C.c_double]),
     "sf_last_solve_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), dp]),
     "sf_get_info": (i32, [vp, C.c_char_p, dp]),
+    "sf_cg_noalloc": (i32, [vp, i32, vp, vp, C.c_double, i32, C.POINTER(i32), dp, vp]),
 }
+
+SF_NOALLOC_MAX_FREE = 262144
 
 for _name, (_res, _args) in SIGNATURES.items():
     _f = getattr(lib, _name)

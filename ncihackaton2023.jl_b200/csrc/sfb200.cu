@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -686,3 +687,127 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres) 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// sf_cg_noalloc: the FP64 CG of sf_cg with its scratch in a static device array.
+//
+// Who needs it: callers that cannot call cudaMalloc. For example, a host
+// whose device memory is owned by its own pool allocator (CUDA.jl's and
+// PyTorch's caching allocators keep freed memory for reuse), or a
+// time-critical loop that cannot afford the device-wide synchronisation
+// cudaMalloc/cudaFree can cause. sf_cg allocates its workspace, the cached
+// diagonal and a pinned host scalar on first use. This variant uses none of
+// them.
+//
+// The scratch (vectors r, p, q, dinv and diag of up to SF_NOALLOC_MAX_FREE
+// dofs, plus the CG scalars and reduction partial sums, about 10 MB) is one
+// file-scope __device__ array. Every GPU that loads this library holds it
+// until the process exits. Its device address is looked up with
+// cudaGetSymbolAddress by the first call on each device, with that device
+// current. All calls share the array, so calls that overlap on the GPU
+// race. Everything a call reads from the array is written by that call
+// first, and the diagonal is re-zeroed on every call before it is
+// accumulated.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr long long kNoAllocMaxFree = SF_NOALLOC_MAX_FREE;
+constexpr long long kNoAllocScalarWords = 32;  // CG scalars, padded to 256 bytes
+constexpr long long kNoAllocWords =
+    5 * kNoAllocMaxFree + kNoAllocScalarWords + 3LL * sf::kRedBlocks;
+static_assert((kNoAllocMaxFree * 8) % 256 == 0, "scratch vectors must stay 256-byte aligned");
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up once per device).
+double* noalloc_scratch() {
+  int dev = -1;
+  SF_CUDA_CHECK(cudaGetDevice(&dev));
+  SF_REQUIRE(dev >= 0 && dev < kNoAllocMaxDevices, SF_ERR_UNSUPPORTED,
+             "device ordinal beyond the no-alloc address table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    SF_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    SF_REQUIRE(p != nullptr, SF_ERR_CUDA, "cudaGetSymbolAddress returned null");
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+double read_scalar_noalloc(const double* d_s, int slot, cudaStream_t st) {
+  double h = 0.0;
+  SF_CUDA_CHECK(cudaMemcpyAsync(&h, d_s + slot, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SF_CUDA_CHECK(cudaStreamSynchronize(st));
+  return h;
+}
+
+int cg_f64_noalloc(sf_op* op, bool jacobi, const double* b, double* x, double reltol, int maxiter,
+                   double* relres, cudaStream_t st) {
+  const long long n = op->n_free;
+  double* base = noalloc_scratch();
+  double* r = base;
+  double* p = base + kNoAllocMaxFree;
+  double* q = base + 2 * kNoAllocMaxFree;
+  double* dinv = base + 3 * kNoAllocMaxFree;
+  double* diag = base + 4 * kNoAllocMaxFree;
+  double* s = base + 5 * kNoAllocMaxFree;
+  double* partials = s + kNoAllocScalarWords;
+  if (jacobi) {
+    SF_CUDA_CHECK(cudaMemsetAsync(diag, 0, n * sizeof(double), st));
+    sf::launch_general_diag(SF_F64, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells,
+                            op->geom, diag, st);
+    sf::vec_invert<double>(diag, dinv, n, st);
+  }
+  const double* Dv = jacobi ? dinv : nullptr;
+  apply_impl(op, SF_F64, x, q, st);
+  sf::cg_start<double>(b, q, Dv, r, p, n, partials, s, st);
+  const double bb = read_scalar_noalloc(s, sf::CG_BB, st);
+  double rr = read_scalar_noalloc(s, sf::CG_RR, st);
+  const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
+  const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
+  int it = 0;
+  while (rr > tol2 && it < maxiter) {
+    apply_impl(op, SF_F64, p, q, st);
+    sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, st);
+    sf::cg_update<double>(s, x, p, r, q, Dv, n, partials, s, st);
+    rr = read_scalar_noalloc(s, sf::CG_RR, st);
+    ++it;
+    SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in CG");
+    if (rr <= tol2) break;
+    sf::cg_direction<double>(s, p, r, Dv, n, st);
+  }
+  *relres = std::sqrt(rr) / nb;
+  return it;
+}
+
+}  // namespace
+
+extern "C" int sf_cg_noalloc(sf_op* op, int mode, const double* b, double* x, double reltol,
+                             int maxiter, int* iters, double* relres, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(b && x, SF_ERR_ARG, "null b or x");
+    SF_REQUIRE(reltol > 0 && maxiter >= 0, SF_ERR_ARG, "bad reltol / maxiter");
+    SF_REQUIRE(op->n_free <= kNoAllocMaxFree, SF_ERR_ARG,
+               "n_free = " + std::to_string(op->n_free) +
+                   " exceeds the no-alloc scratch limit SF_NOALLOC_MAX_FREE = " +
+                   std::to_string(kNoAllocMaxFree));
+    SF_REQUIRE(mode == SF_CG_F64 || mode == SF_CG_F64_PLAIN, SF_ERR_UNSUPPORTED,
+               "sf_cg_noalloc supports SF_CG_F64 and SF_CG_F64_PLAIN only");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double rel = 0.0;
+    const int it = cg_f64_noalloc(op, mode == SF_CG_F64, b, x, reltol, maxiter, &rel, st);
+    op->last_inner = it;
+    op->last_outer = 1;
+    op->last_relres = rel;
+    if (iters) *iters = it;
+    if (relres) *relres = rel;
+    if (!(rel <= reltol)) throw Error(SF_ERR_NOT_CONVERGED, "CG reached its iteration cap");
+  });
+}

@@ -1,0 +1,74 @@
+"""sf_cg_noalloc: the CG entry point for callers that cannot allocate device
+memory (for example, a host whose pool allocator owns the device memory).
+
+It is called through the C ABI and compared with sf_cg, which allocates its
+workspace. The comparison runs twice in a row, because the static scratch
+array keeps the previous call's contents. FP64 tolerance 1e-12 relative.
+This file is named so that pytest collects it last."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import sumfac_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(sf, p, deg, n, gather):
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n))
+    V = sf.FESpace(model, p)
+    m = sf.SumFactorizationMap(3, (p,) * 3, (deg,) * 3)
+    A = sf.LazyMatrix(m, V, V, sf.Measure(model, deg), gather=gather)
+    om = O.make_map(3, p, deg)
+    b = O.rhs(om, O.cartesian_mesh(3, n, p, om), O.sin_forcing)
+    return A, b
+
+
+def _cg_noalloc(A, mode, b, x, reltol, maxiter):
+    import torch
+    from ncihackaton2023_b200 import _lib
+    it, rel = C.c_int(), C.c_double()
+    st = _lib.lib.sf_cg_noalloc(A._h, mode, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+                                float(reltol), int(maxiter), C.byref(it), C.byref(rel),
+                                C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return st, it.value, rel.value
+
+
+@pytest.mark.parametrize("mode,gather,p,deg,n", [("jacobi", "structured", 2, 4, 6),
+                                                ("jacobi", "table", 3, 6, 4),
+                                                ("plain", "structured", 4, 8, 3)])
+def test_cg_noalloc_matches_cg(sf, mode, gather, p, deg, n):
+    import torch
+    from ncihackaton2023_b200 import _lib
+    A, b_np = _problem(sf, p, deg, n, gather)
+    b = torch.from_numpy(b_np).cuda()
+    code = _lib.SF_CG_F64 if mode == "jacobi" else _lib.SF_CG_F64_PLAIN
+    x_ref, info = sf.cg(A, b, reltol=1e-10, mode=mode)
+    for _ in range(2):  # two calls in a row share (and reuse) the scratch array
+        x = torch.zeros_like(b)
+        st, it, rel = _cg_noalloc(A, code, b, x, 1e-10, A.n)
+        assert st == _lib.SF_OK, _lib.lib.sf_last_error(A._h)
+        assert it == info["iters"] and rel <= 1e-10
+        err = ((x - x_ref).abs().max() / x_ref.abs().max()).item()
+        assert err < 1e-12
+
+
+def test_cg_noalloc_rejects_large_and_mixed(sf):
+    import torch
+    from ncihackaton2023_b200 import _lib
+    n = 33  # Q2 on 33^3 cells: 65^3 = 274625 free dofs > SF_NOALLOC_MAX_FREE
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n))
+    V = sf.FESpace(model, 2)
+    m = sf.SumFactorizationMap(3, (2,) * 3, (4,) * 3)
+    A = sf.LazyMatrix(m, V, V, sf.Measure(model, 4))
+    assert A.n > _lib.SF_NOALLOC_MAX_FREE
+    b = torch.ones(A.n, dtype=torch.float64, device="cuda")
+    x = torch.zeros_like(b)
+    st, _, _ = _cg_noalloc(A, _lib.SF_CG_F64, b, x, 1e-10, 10)
+    assert st == _lib.SF_ERR_ARG
+    assert b"SF_NOALLOC_MAX_FREE" in _lib.lib.sf_last_error(A._h)
+    A2, b2 = _problem(sf, 2, 4, 3, "structured")
+    bd = torch.from_numpy(b2).cuda()
+    st, _, _ = _cg_noalloc(A2, _lib.SF_CG_MIXED, bd, torch.zeros_like(bd), 1e-10, 10)
+    assert st == _lib.SF_ERR_UNSUPPORTED
