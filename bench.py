@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--tile", type=int, default=None,
+                    help="force tile candidate K of the FP64 tiled kernel (skips the autotuner)")
     ap.add_argument("--cells", type=int, default=64,
                     help="cells per direction (64 is the benchmark; smaller only for profiling)")
     a = ap.parse_args()
@@ -163,6 +165,29 @@ def cpu_baseline_port(nsteps_full=3):
                       f"reference loops (oracle/sumfac_ref.c), 1 thread; {t:.3f} s per apply"}
 
 
+def time_tile_candidates(A, dev, reps=20):
+    """ms per apply of every tile shape of the tiled kernel (FP64 and FP32)."""
+    import torch
+    out = {}
+    for dt, key in ((torch.float64, "f64"), (torch.float32, "f32")):
+        nc = int(A.info(f"tile_candidates_{key}"))
+        x = torch.zeros(A.n, dtype=dt, device=dev)
+        y = torch.empty_like(x)
+        for k in range(nc):
+            A.set_option(f"tile_candidate_{key}", k)
+            for _ in range(3):
+                A @ x
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                from __graft_entry__ import load
+                load().mul(y, A, x)
+            e1.record()
+            torch.cuda.synchronize()
+            out[f"{key}: {A.kernel_name(dt)}"] = round(e0.elapsed_time(e1) / reps, 4)
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -172,6 +197,13 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     m, model, V, A = build_problem(sf)
+    tile_ms = {}
+    if args.tile is not None:
+        A.set_option("tile_candidate_f64", args.tile)
+        tuned = {"f64": A.kernel_name(torch.float64), "f32": A.kernel_name(torch.float32)}
+    else:
+        tile_ms = time_tile_candidates(A, dev)
+        tuned = {"f64": A.autotune(torch.float64), "f32": A.autotune(torch.float32)}
     n = V.num_free_dofs
     rng = np.random.default_rng(0 + rank)
     x0 = torch.from_numpy(rng.uniform(-1, 1, n)).to(dev)
@@ -242,6 +274,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic: x ~ U[-1,1] seed 0 (rank r: seed r)",
         "config": {"workload": WORKLOAD, "n_cells": NCELL ** 3, "order": P, "quad_points": 5,
                    "n_dof_total": N_DOF_TOTAL, "n_free": n, "kernel": kernel_path,
+                   "tile": tuned, "tile_ms": tile_ms,
                    "l2": "4 rotating x/y pairs (1.09 GB) > 126 MB L2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": e2e,

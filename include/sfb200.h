@@ -156,6 +156,8 @@ int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int ma
  *   "mixed_inner_reltol" : SF_CG_MIXED refines (FP64 true residual replaces the FP32
  *                          recurrence residual) each time the FP32 residual has
  *                          dropped by this factor (default 0.1)
+ *   "tile_candidate_f64"  : force tile-shape candidate k of the tiled Cartesian kernel
+ *   "tile_candidate_f32"    (0-based; see sf_get_info "tile_candidates_f64/f32")
  */
 int sf_set_option(sf_op* op, const char* name, double value);
 
@@ -168,8 +170,22 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *   "tiled_kernel"           : 1 if sf_apply(SF_F64) uses the tiled Cartesian kernel
  *   "kernels_per_apply"      : kernel launches one sf_apply(SF_F64) makes
  *   "geometry_kind"          : 1 separable constant metric, 2 per-point table
+ *   "tile_candidates_f64/f32": number of tile shapes of the tiled kernel (0 if not in use)
  */
 int sf_get_info(const sf_op* op, const char* key, double* value);
+
+/*
+ * Time every tile-shape candidate of the tiled Cartesian kernel for this
+ * handle's order, mesh and dtype, and keep the fastest for later sf_apply
+ * calls. Temporary x / y buffers are allocated for the timing. Without the
+ * tiled kernel (table gather, deformed cells, kappa) it does nothing.
+ * Replaces the launch-configuration table that the reference kept by hand
+ * (test/benchmark_v3.jl:36-40).
+ */
+int sf_autotune(sf_op* op, int dtype, void* stream);
+
+/* Description of the kernel sf_apply uses for dtype (static string). */
+const char* sf_kernel_name(const sf_op* op, int dtype);
 
 /*
  * sf_cg_noalloc: sf_cg without any device or pinned-host allocation. It has no

@@ -62,6 +62,8 @@ SIGNATURES = {
     "sf_last_solve_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), dp]),
     "sf_get_info": (i32, [vp, C.c_char_p, dp]),
     "sf_cg_noalloc": (i32, [vp, i32, vp, vp, C.c_double, i32, C.POINTER(i32), dp, vp]),
+    "sf_autotune": (i32, [vp, i32, vp]),
+    "sf_kernel_name": (C.c_char_p, [vp, i32]),
 }
 
 SF_NOALLOC_MAX_FREE = 262144

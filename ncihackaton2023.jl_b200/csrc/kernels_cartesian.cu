@@ -158,11 +158,17 @@ struct Acc {  // even/odd accumulators of one output line
   }
 };
 
-template <int P, int EX, int EY, int EZ>
+template <int P, int EX, int EY, int EZ, typename T>
 struct Tile {
   static constexpr int BX = (EX + 1) * P + 1, BY = (EY + 1) * P + 1, BZ = (EZ + 1) * P + 1;
   static constexpr int OX = EX * P, OY = EY * P, OZ = EZ * P;
-  static constexpr int PLANE = BX * BY;
+  // Plane stride padded so that PLANE = BX (mod M), M = words per bank sweep (16
+  // doubles / 32 floats). The y pass gives consecutive lanes consecutive x, and a
+  // request that wraps from one z-plane into the next then maps onto the banks as
+  // if the rows were contiguous, so it has no bank conflicts.
+  static constexpr int M = sizeof(T) == 8 ? 16 : 32;
+  static constexpr int PAD = ((BX - BX * BY) % M + M) % M;
+  static constexpr int PLANE = BX * BY + PAD;
   static constexpr int TS = PLANE * OZ;  // each of t1 (-> a -> y) and t2 (-> s)
   static constexpr int WORDS = 2 * TS;
 };
@@ -221,7 +227,7 @@ __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body&
 template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
 k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
-  using G = Tile<P, EX, EY, EZ>;
+  using G = Tile<P, EX, EY, EZ, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* T1 = reinterpret_cast<T*>(smem_raw);  // t1 -> a -> y   [OZ][BY][BX]
   T* T2 = T1 + G::TS;                        // t2 -> s        [OZ][BY][BX]
@@ -339,32 +345,6 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   }
 }
 
-// Tile shapes per (P, dtype). Shared memory is 2 * (E*P+P+1)^2 * EZ*P words.
-template <int P, typename T>
-struct Config;
-#define SF_CART_CONFIG(P_, T_, EX_, EY_, EZ_, NT_, MINB_)                   \
-  template <>                                                               \
-  struct Config<P_, T_> {                                                   \
-    static constexpr int EX = EX_, EY = EY_, EZ = EZ_, NT = NT_, MINB = MINB_; \
-  };
-SF_CART_CONFIG(1, double, 8, 8, 4, 256, 2)
-SF_CART_CONFIG(2, double, 4, 4, 4, 256, 2)
-SF_CART_CONFIG(3, double, 4, 4, 2, 256, 2)
-SF_CART_CONFIG(4, double, 4, 4, 2, 256, 3)
-SF_CART_CONFIG(5, double, 2, 2, 2, 256, 2)
-SF_CART_CONFIG(6, double, 2, 2, 2, 256, 1)
-SF_CART_CONFIG(7, double, 2, 2, 1, 256, 1)
-SF_CART_CONFIG(8, double, 2, 2, 1, 256, 1)
-SF_CART_CONFIG(1, float, 8, 8, 4, 256, 2)
-SF_CART_CONFIG(2, float, 4, 4, 4, 256, 2)
-SF_CART_CONFIG(3, float, 4, 4, 4, 256, 2)
-SF_CART_CONFIG(4, float, 4, 4, 2, 256, 3)
-SF_CART_CONFIG(5, float, 2, 2, 2, 256, 2)
-SF_CART_CONFIG(6, float, 2, 2, 2, 256, 2)
-SF_CART_CONFIG(7, float, 2, 2, 2, 256, 2)
-SF_CART_CONFIG(8, float, 2, 2, 1, 256, 2)
-#undef SF_CART_CONFIG
-
 template <int P, typename T>
 void fill_eo(const double* M, double scale, T* ue, T* uo) {
   using S = EO<P>;
@@ -380,10 +360,10 @@ void fill_eo(const double* M, double scale, T* ue, T* uo) {
     for (int j = i; j < S::NO; ++j) uo[tri(i, j, S::NO)] = (T)(0.5 * (m(i, j) - m(i, P - j)));
 }
 
-template <int P, typename T>
-void run_cartesian(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st) {
-  using C = Config<P, T>;
-  using G = Tile<P, C::EX, C::EY, C::EZ>;
+// One launch of the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
+template <int P, typename T, int EX, int EY, int EZ, int NT, int MINB>
+void run_tile(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st) {
+  using G = Tile<P, EX, EY, EZ, T>;
   CartParams<P, T> Q{};
   fill_eo<P, T>(plan.M, 1.0, Q.Me, Q.Mo);
   fill_eo<P, T>(plan.K, 1.0, Q.Ke, Q.Ko);
@@ -397,37 +377,96 @@ void run_cartesian(const CartesianPlan& plan, const void* x, void* y, cudaStream
   Q.nfx = plan.nx * P - 1;
   Q.nfy = plan.ny * P - 1;
   Q.nfz = plan.nz * P - 1;
-  Q.ntx = (plan.nx + C::EX - 1) / C::EX;
-  Q.nty = (plan.ny + C::EY - 1) / C::EY;
-  Q.ntz = (plan.nz + C::EZ - 1) / C::EZ;
+  Q.ntx = (plan.nx + EX - 1) / EX;
+  Q.nty = (plan.ny + EY - 1) / EY;
+  Q.ntz = (plan.nz + EZ - 1) / EZ;
   const long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
   SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
   const size_t smem = (size_t)G::WORDS * sizeof(T);
   if (iso) {
-    auto kern = k_cartesian<P, C::EX, C::EY, C::EZ, C::NT, true, T, C::MINB>;
+    auto kern = k_cartesian<P, EX, EY, EZ, NT, true, T, MINB>;
     SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(unsigned)tiles, C::NT, smem, st>>>(Q);
+    kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
   } else {
-    auto kern = k_cartesian<P, C::EX, C::EY, C::EZ, C::NT, false, T, C::MINB>;
+    auto kern = k_cartesian<P, EX, EY, EZ, NT, false, T, MINB>;
     SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(unsigned)tiles, C::NT, smem, st>>>(Q);
+    kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
   }
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
+using RunFn = void (*)(const CartesianPlan&, const void*, void*, cudaStream_t);
+struct Candidate {
+  RunFn run;
+  const char* name;
+};
+#define SF_TILE(P_, T_, EX_, EY_, EZ_, NT_, MINB_) \
+  {&run_tile<P_, T_, EX_, EY_, EZ_, NT_, MINB_>, #EX_ "x" #EY_ "x" #EZ_ " cells, " #NT_ " thr, " #MINB_ "/SM"}
+
+// Candidate tile shapes per (P, dtype); the first is the default. Shared
+// memory per CTA is 2 * PLANE * EZ*P words. The autotuner times them all on
+// the operator's own mesh.
+template <int P, typename T>
+struct Cands;
+template <> struct Cands<1, double> { static constexpr Candidate c[] = {SF_TILE(1, double, 8, 8, 4, 256, 2)}; };
+template <> struct Cands<2, double> { static constexpr Candidate c[] = {SF_TILE(2, double, 4, 4, 4, 256, 2),
+                                                                      SF_TILE(2, double, 8, 4, 2, 256, 2)}; };
+template <> struct Cands<3, double> { static constexpr Candidate c[] = {SF_TILE(3, double, 4, 4, 2, 256, 2),
+                                                                      SF_TILE(3, double, 4, 4, 3, 256, 2)}; };
+template <> struct Cands<4, double> { static constexpr Candidate c[] = {SF_TILE(4, double, 4, 4, 2, 256, 3),
+                                                                      SF_TILE(4, double, 4, 4, 3, 256, 2),
+                                                                      SF_TILE(4, double, 4, 4, 4, 256, 2),
+                                                                      SF_TILE(4, double, 4, 4, 2, 224, 3),
+                                                                      SF_TILE(4, double, 4, 4, 3, 320, 2)}; };
+template <> struct Cands<5, double> { static constexpr Candidate c[] = {SF_TILE(5, double, 2, 2, 2, 256, 2)}; };
+template <> struct Cands<6, double> { static constexpr Candidate c[] = {SF_TILE(6, double, 2, 2, 2, 256, 1)}; };
+template <> struct Cands<7, double> { static constexpr Candidate c[] = {SF_TILE(7, double, 2, 2, 1, 256, 1)}; };
+template <> struct Cands<8, double> { static constexpr Candidate c[] = {SF_TILE(8, double, 2, 2, 1, 256, 1)}; };
+template <> struct Cands<1, float> { static constexpr Candidate c[] = {SF_TILE(1, float, 8, 8, 4, 256, 2)}; };
+template <> struct Cands<2, float> { static constexpr Candidate c[] = {SF_TILE(2, float, 4, 4, 4, 256, 2)}; };
+template <> struct Cands<3, float> { static constexpr Candidate c[] = {SF_TILE(3, float, 4, 4, 4, 256, 2),
+                                                                     SF_TILE(3, float, 4, 4, 2, 256, 3)}; };
+template <> struct Cands<4, float> { static constexpr Candidate c[] = {SF_TILE(4, float, 4, 4, 2, 256, 3),
+                                                                     SF_TILE(4, float, 4, 4, 3, 256, 3),
+                                                                     SF_TILE(4, float, 4, 4, 4, 256, 3),
+                                                                     SF_TILE(4, float, 4, 4, 3, 256, 4)}; };
+template <> struct Cands<5, float> { static constexpr Candidate c[] = {SF_TILE(5, float, 2, 2, 2, 256, 2)}; };
+template <> struct Cands<6, float> { static constexpr Candidate c[] = {SF_TILE(6, float, 2, 2, 2, 256, 2)}; };
+template <> struct Cands<7, float> { static constexpr Candidate c[] = {SF_TILE(7, float, 2, 2, 2, 256, 2)}; };
+template <> struct Cands<8, float> { static constexpr Candidate c[] = {SF_TILE(8, float, 2, 2, 1, 256, 2)}; };
+#undef SF_TILE
+
+template <typename T, int P>
+int cand_count() { return (int)(sizeof(Cands<P, T>::c) / sizeof(Candidate)); }
+
 template <typename T>
-void dispatch(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st) {
-  switch (plan.SB - 1) {
-    case 1: return run_cartesian<1, T>(plan, x, y, st);
-    case 2: return run_cartesian<2, T>(plan, x, y, st);
-    case 3: return run_cartesian<3, T>(plan, x, y, st);
-    case 4: return run_cartesian<4, T>(plan, x, y, st);
-    case 5: return run_cartesian<5, T>(plan, x, y, st);
-    case 6: return run_cartesian<6, T>(plan, x, y, st);
-    case 7: return run_cartesian<7, T>(plan, x, y, st);
-    case 8: return run_cartesian<8, T>(plan, x, y, st);
+const Candidate& candidate(int SB, int k) {
+  switch (SB - 1) {
+#define SF_CASE(P_) \
+  case P_: return Cands<P_, T>::c[k < cand_count<T, P_>() ? k : 0];
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
     default: throw Error(SF_ERR_UNSUPPORTED, "no tiled Cartesian kernel for this order");
   }
+}
+
+template <typename T>
+int candidates_for(int SB) {
+  switch (SB - 1) {
+#define SF_CASE(P_) \
+  case P_: return cand_count<T, P_>();
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+    default: return 0;
+  }
+}
+
+int candidate_count(int SB, int dtype) {
+  return dtype == SF_F64 ? candidates_for<double>(SB) : candidates_for<float>(SB);
+}
+
+const Candidate& pick(const CartesianPlan& plan, int dtype, int k) {
+  return dtype == SF_F64 ? candidate<double>(plan.SB, k) : candidate<float>(plan.SB, k);
 }
 
 }  // namespace
@@ -481,12 +520,32 @@ bool cartesian_supported(const CartesianPlan& plan, int dtype) {
 
 int cartesian_launches(const CartesianPlan& plan) { return 1; }
 
+static int dtype_slot(int dtype) {
+  if (dtype == SF_F64) return 0;
+  if (dtype == SF_F32) return 1;
+  throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
+}
+
+int cartesian_candidates(const CartesianPlan& plan, int dtype) {
+  dtype_slot(dtype);
+  return candidate_count(plan.SB, dtype);
+}
+
+const char* cartesian_candidate_name(const CartesianPlan& plan, int dtype, int k) {
+  dtype_slot(dtype);
+  return pick(plan, dtype, k).name;
+}
+
+void cartesian_apply_candidate(const CartesianPlan& plan, int dtype, int k, const void* x, void* y,
+                               cudaStream_t stream) {
+  SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
+  dtype_slot(dtype);
+  pick(plan, dtype, k).run(plan, x, y, stream);
+}
+
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
                      cudaStream_t stream) {
-  SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
-  if (dtype == SF_F64) dispatch<double>(plan, x, y, stream);
-  else if (dtype == SF_F32) dispatch<float>(plan, x, y, stream);
-  else throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
+  cartesian_apply_candidate(plan, dtype, plan.choice[dtype_slot(dtype)], x, y, stream);
 }
 
 void cartesian_release(CartesianPlan& plan) { plan.ready = false; }

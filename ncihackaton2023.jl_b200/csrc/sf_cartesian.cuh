@@ -12,12 +12,18 @@ struct CartesianPlan {
   double M[kMaxSB * kMaxSB] = {0};  // 1D element mass A^T W A, lexicographic order
   double K[kMaxSB * kMaxSB] = {0};  // 1D element stiffness B^T W B
   double c[3] = {0, 0, 0};          // G0 diagonal: xx, yy, zz
+  int choice[2] = {0, 0};           // tile candidate per dtype (0: FP64, 1: FP32)
 };
 
 // Builds the 1D operators; returns false when no tiled kernel exists for SB.
 bool cartesian_prepare(CartesianPlan& plan, int SB, int SQ, const double* A, const double* B,
                        const double* w1, const double* G0, int nx, int ny, int nz);
 bool cartesian_supported(const CartesianPlan& plan, int dtype);
+// Tile-shape candidates for the plan's order and dtype (timed by sf_autotune).
+int cartesian_candidates(const CartesianPlan& plan, int dtype);
+const char* cartesian_candidate_name(const CartesianPlan& plan, int dtype, int k);
+void cartesian_apply_candidate(const CartesianPlan& plan, int dtype, int k, const void* x, void* y,
+                               cudaStream_t stream);
 int cartesian_launches(const CartesianPlan& plan);  // kernel launches per apply
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
                      cudaStream_t stream);

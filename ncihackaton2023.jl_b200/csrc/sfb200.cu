@@ -659,10 +659,73 @@ int sf_set_option(sf_op* op, const char* name, double value) {
     if (n == "mixed_inner_reltol") {
       SF_REQUIRE(value > 0 && value < 1, SF_ERR_ARG, "mixed_inner_reltol must be in (0,1)");
       op->mixed_inner_reltol = value;
+    } else if (n == "tile_candidate_f64" || n == "tile_candidate_f32") {
+      const int dt = n == "tile_candidate_f64" ? SF_F64 : SF_F32;
+      SF_REQUIRE(op->cartesian_ok, SF_ERR_STATE, "the tiled Cartesian kernel is not in use");
+      const int nc = sf::cartesian_candidates(op->cart, dt);
+      SF_REQUIRE(value >= 0 && value < nc && value == (int)value, SF_ERR_ARG,
+                 "tile candidate out of range (0.." + std::to_string(nc - 1) + ")");
+      op->cart.choice[dt == SF_F64 ? 0 : 1] = (int)value;
     } else {
       throw Error(SF_ERR_ARG, "unknown option " + n);
     }
   });
+}
+
+int sf_autotune(sf_op* op, int dtype, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    const size_t es = dsize(dtype);
+    if (!(op->cartesian_ok && sf::cartesian_supported(op->cart, dtype)) || op->n_free == 0) return;
+    const int nc = sf::cartesian_candidates(op->cart, dtype);
+    if (nc <= 1) return;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    void* x = nullptr;
+    void* y = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&] {
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+      if (x) cudaFree(x);
+      if (y) cudaFree(y);
+    };
+    try {
+      SF_CUDA_CHECK(cudaMalloc(&x, op->n_free * es));
+      SF_CUDA_CHECK(cudaMalloc(&y, op->n_free * es));
+      SF_CUDA_CHECK(cudaMemsetAsync(x, 0, op->n_free * es, st));
+      SF_CUDA_CHECK(cudaEventCreate(&e0));
+      SF_CUDA_CHECK(cudaEventCreate(&e1));
+      int best = 0;
+      float best_ms = 0.f;
+      for (int k = 0; k < nc; ++k) {
+        for (int w = 0; w < 2; ++w) sf::cartesian_apply_candidate(op->cart, dtype, k, x, y, st);
+        SF_CUDA_CHECK(cudaEventRecord(e0, st));
+        for (int r = 0; r < 5; ++r) sf::cartesian_apply_candidate(op->cart, dtype, k, x, y, st);
+        SF_CUDA_CHECK(cudaEventRecord(e1, st));
+        SF_CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        SF_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        if (k == 0 || ms < best_ms) {
+          best = k;
+          best_ms = ms;
+        }
+      }
+      op->cart.choice[dtype == SF_F64 ? 0 : 1] = best;
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
+  });
+}
+
+const char* sf_kernel_name(const sf_op* op, int dtype) {
+  if (!op) return "null handle";
+  if (dtype != SF_F64 && dtype != SF_F32) return "invalid dtype";
+  if (op->cartesian_ok && sf::cartesian_supported(op->cart, dtype))
+    return sf::cartesian_candidate_name(op->cart, dtype, op->cart.choice[dtype == SF_F64 ? 0 : 1]);
+  return "general element kernel";
 }
 
 int sf_get_info(const sf_op* op, const char* key, double* value) {
@@ -674,6 +737,11 @@ int sf_get_info(const sf_op* op, const char* key, double* value) {
   else if (k == "tiled_kernel") *value = tiled ? 1.0 : 0.0;
   else if (k == "kernels_per_apply") *value = tiled ? (double)sf::cartesian_launches(op->cart) : 1.0;
   else if (k == "geometry_kind") *value = (double)op->geom.kind;
+  else if (k == "tile_candidates_f64" || k == "tile_candidates_f32") {
+    const int dt = k == "tile_candidates_f64" ? SF_F64 : SF_F32;
+    *value = (op->cartesian_ok && sf::cartesian_supported(op->cart, dt))
+                 ? (double)sf::cartesian_candidates(op->cart, dt) : 0.0;
+  }
   else return SF_ERR_ARG;
   return SF_OK;
 }

@@ -212,6 +212,17 @@ class LazyMatrix:
         check(lib.sf_get_info(self._h, key.encode(), C.byref(v)), self._h, "sf_get_info")
         return v.value
 
+    def autotune(self, dtype=None):
+        """Time the tiled kernel's tile-shape candidates on this mesh and keep the
+        fastest (no-op when the general element kernel is in use)."""
+        dtype = dtype or torch.float64
+        check(lib.sf_autotune(self._h, _dtype_code(dtype), _stream()), self._h, "sf_autotune")
+        return self.kernel_name(dtype)
+
+    def kernel_name(self, dtype=None) -> str:
+        dtype = dtype or torch.float64
+        return lib.sf_kernel_name(self._h, _dtype_code(dtype)).decode()
+
     def uses_tiled_kernel(self) -> bool:
         return self.info("tiled_kernel") == 1.0
 

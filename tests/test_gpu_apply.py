@@ -69,6 +69,30 @@ def test_all_orders(sf, p):
         assert relerr(y, y_ref) < TOL64, (p, deg)
 
 
+@pytest.mark.parametrize("p,deg", [(2, 4), (3, 6), (4, 8), (4, 6)])
+def test_every_tile_candidate(sf, p, deg):
+    """Every tile shape the autotuner may pick gives the oracle's result, on a
+    mesh that is not a multiple of any tile (partial tiles at the far faces)."""
+    torch = _torch()
+    n = (5, 6, 7)
+    A, V = build(sf, p, deg, n)
+    om = O.make_map(3, p, deg)
+    mesh = O.cartesian_mesh(3, n, p, om)
+    x = np.random.default_rng(p).uniform(-1, 1, mesh.n_free)
+    y_ref = O.lazy_mul(om, mesh, x)
+    xd = torch.from_numpy(x).cuda()
+    for dt, tol, key in ((torch.float64, TOL64, "f64"), (torch.float32, TOL32, "f32")):
+        ncand = int(A.info(f"tile_candidates_{key}"))
+        assert ncand >= 1
+        for k in range(ncand):
+            A.set_option(f"tile_candidate_{key}", k)
+            y = (A @ xd.to(dt)).double().cpu().numpy()
+            assert relerr(y, y_ref) < tol, (key, k, A.kernel_name(dt))
+        name = A.autotune(dt)
+        y = (A @ xd.to(dt)).double().cpu().numpy()
+        assert relerr(y, y_ref) < tol, name
+
+
 def test_renumbered_table(sf):
     torch = _torch()
     p, deg, n = 3, 6, 4
