@@ -112,6 +112,20 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
  * NULL for kappa = 1. The operator becomes -div(kappa grad u). */
 int sf_set_coefficient(sf_op* op, const double* kappa);
 
+/* Same, from a DEVICE array (ncells x SQ^D FP64), copied on `stream`. */
+int sf_set_coefficient_device(sf_op* op, const double* kappa, void* stream);
+
+/*
+ * Vector-Jacobian product of y = A(kappa) x with respect to kappa (device
+ * pointers): kappa_bar[c][q] = (grad ybar)_q^T G_q (grad x)_q, where G = wq*djq*jq^T*jq
+ * is the reference's per-point metric (src/SumFactorizationKernels.jl:174-216)
+ * without kappa. The gradients are recomputed by sum factorization and not
+ * stored. kappa_bar is ncells x SQ^D FP64; x, ybar are n_free of dtype.
+ * The product with respect to x is sf_apply(ybar), because A is symmetric.
+ */
+int sf_kappa_vjp(sf_op* op, int dtype, const void* x, const void* ybar, double* kappa_bar,
+                 void* stream);
+
 /*
  * y = A x over the free dofs, device pointers, enqueued on `stream`
  * (a cudaStream_t, NULL = legacy default). Replaces

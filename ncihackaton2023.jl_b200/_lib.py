@@ -63,6 +63,8 @@ SIGNATURES = {
     "sf_get_info": (i32, [vp, C.c_char_p, dp]),
     "sf_cg_noalloc": (i32, [vp, i32, vp, vp, C.c_double, i32, C.POINTER(i32), dp, vp]),
     "sf_autotune": (i32, [vp, i32, vp]),
+    "sf_set_coefficient_device": (i32, [vp, vp, vp]),
+    "sf_kappa_vjp": (i32, [vp, i32, vp, vp, vp, vp]),
     "sf_kernel_name": (C.c_char_p, [vp, i32]),
 }
 

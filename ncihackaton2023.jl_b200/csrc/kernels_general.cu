@@ -319,6 +319,160 @@ __global__ void k_general_diag(const __grid_constant__ GenParams<SB, SQ, T> P) {
   atomicAdd(P.y + id, (T)acc);
 }
 
+// ---------------------------------------------------------------------------
+// Vector-Jacobian product of y = A(kappa) x with respect to kappa:
+//   kappa_bar[c][q] = (grad ybar)_q^T G_q (grad x)_q
+// with G = wq djq jq^T jq (without kappa). This is the derivative of ybar^T A(kappa) x
+// with respect to kappa_q, the per-point factor of the reference's apply_weights
+// (src/SumFactorizationKernels.jl:174-216). The gradients at the points are
+// recomputed by sum factorization for both vectors, one element per
+// max(SB,SQ)^2 threads, and never stored in global memory. Nothing is scattered.
+// ---------------------------------------------------------------------------
+template <int SB, int SQ>
+struct VjpShape {
+  using S = Shape<SB, SQ>;
+  static constexpr int SE = 2 * (S::S0 + 2 * S::S1 + 3 * S::S2);  // x and ybar buffers
+  static constexpr int EPB = (128 / S::NL) > 0 ? (128 / S::NL) : 1;
+  static constexpr int THREADS = EPB * S::NL;
+};
+
+// forward passes x/y of the element kernel: X -> (A1, B1) -> (AA, AB, BA)
+template <int SB, int SQ, typename T>
+__device__ __forceinline__ void forward_xy(const GenParams<SB, SQ, T>& P, int l, const T* X, T* A1,
+                                           T* B1, T* AA, T* AB, T* BA) {
+  if (l < SB * SB) {
+    T in[SB];
+#pragma unroll
+    for (int i = 0; i < SB; ++i) in[i] = X[l * SB + i];
+#pragma unroll
+    for (int qi = 0; qi < SQ; ++qi) {
+      T a = T(0), b = T(0);
+#pragma unroll
+      for (int i = 0; i < SB; ++i) {
+        a = fma(P.A[qi * SB + i], in[i], a);
+        b = fma(P.B[qi * SB + i], in[i], b);
+      }
+      A1[l * SQ + qi] = a;
+      B1[l * SQ + qi] = b;
+    }
+  }
+  __syncthreads();
+  if (l < SQ * SB) {
+    const int qi = l % SQ, k = l / SQ;
+    T a1[SB], b1[SB];
+#pragma unroll
+    for (int j = 0; j < SB; ++j) {
+      a1[j] = A1[(k * SB + j) * SQ + qi];
+      b1[j] = B1[(k * SB + j) * SQ + qi];
+    }
+#pragma unroll
+    for (int qj = 0; qj < SQ; ++qj) {
+      T aa = T(0), ab = T(0), ba = T(0);
+#pragma unroll
+      for (int j = 0; j < SB; ++j) {
+        aa = fma(P.A[qj * SB + j], a1[j], aa);
+        ab = fma(P.B[qj * SB + j], a1[j], ab);
+        ba = fma(P.A[qj * SB + j], b1[j], ba);
+      }
+      const int o = (k * SQ + qj) * SQ + qi;
+      AA[o] = aa;
+      AB[o] = ab;
+      BA[o] = ba;
+    }
+  }
+}
+
+template <int SB, int SQ, typename T>
+__global__ void __launch_bounds__(VjpShape<SB, SQ>::THREADS)
+k_kappa_vjp(const __grid_constant__ GenParams<SB, SQ, T> P, const T* __restrict__ ybar,
+            double* __restrict__ kbar) {
+  using S = Shape<SB, SQ>;
+  using V = VjpShape<SB, SQ>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int el = threadIdx.x / S::NL;
+  const int l = threadIdx.x % S::NL;
+  const long long cell = (long long)blockIdx.x * V::EPB + el;
+  const bool valid = cell < P.ncells;
+  T* base = reinterpret_cast<T*>(smem_raw) + (size_t)el * V::SE;
+  T* buf[2][6];
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    T* b = base + v * (V::SE / 2);
+    buf[v][0] = b;                        // X
+    buf[v][1] = b + S::S0;                // A1
+    buf[v][2] = buf[v][1] + S::S1;        // B1
+    buf[v][3] = buf[v][2] + S::S1;        // AA
+    buf[v][4] = buf[v][3] + S::S2;        // AB
+    buf[v][5] = buf[v][4] + S::S2;        // BA
+  }
+  // gather x and ybar
+  for (int pos = l; pos < S::S0; pos += S::NL) {
+    T vx = T(0), vy = T(0);
+    if (valid) {
+      long long id;
+      if (P.ids) id = P.ids[cell * S::S0 + pos];
+      else id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+      if (id >= 0) {
+        vx = P.x[id];
+        vy = ybar[id];
+      }
+    }
+    buf[0][0][pos] = vx;
+    buf[1][0][pos] = vy;
+  }
+  __syncthreads();
+  forward_xy<SB, SQ, T>(P, l, buf[0][0], buf[0][1], buf[0][2], buf[0][3], buf[0][4], buf[0][5]);
+  forward_xy<SB, SQ, T>(P, l, buf[1][0], buf[1][1], buf[1][2], buf[1][3], buf[1][4], buf[1][5]);
+  __syncthreads();
+  if (l < SQ * SQ && valid) {
+    const int qi = l % SQ, qj = l / SQ;
+    T c[2][3][SB];  // [vector][BA, AB, AA][k]
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+#pragma unroll
+      for (int k = 0; k < SB; ++k) {
+        const int o = (k * SQ + qj) * SQ + qi;
+        c[v][0][k] = buf[v][5][o];
+        c[v][1][k] = buf[v][4][o];
+        c[v][2][k] = buf[v][3][o];
+      }
+#pragma unroll
+    for (int qk = 0; qk < SQ; ++qk) {
+      double g[2][3];
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        T gx = T(0), gy = T(0), gz = T(0);
+#pragma unroll
+        for (int k = 0; k < SB; ++k) {
+          gx = fma(P.A[qk * SB + k], c[v][0][k], gx);
+          gy = fma(P.A[qk * SB + k], c[v][1][k], gy);
+          gz = fma(P.B[qk * SB + k], c[v][2][k], gz);
+        }
+        g[v][0] = (double)gx;
+        g[v][1] = (double)gy;
+        g[v][2] = (double)gz;
+      }
+      const int q = qi + SQ * (qj + SQ * qk);
+      double G[6];
+      if (P.geom == GEOM_SEPARABLE) {
+        const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) G[m] = s * P.G0[m];
+      } else {
+        const double* gt = P.gtab + cell * P.gstride;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) G[m] = gt[m * SQ * SQ * SQ + q];
+      }
+      const double* u = g[0];
+      const double* w = g[1];
+      const double gu0 = G[0] * u[0] + G[3] * u[1] + G[4] * u[2];
+      const double gu1 = G[3] * u[0] + G[1] * u[1] + G[5] * u[2];
+      const double gu2 = G[4] * u[0] + G[5] * u[1] + G[2] * u[2];
+      kbar[cell * (SQ * SQ * SQ) + q] = w[0] * gu0 + w[1] * gu1 + w[2] * gu2;
+    }
+  }
+}
+
 template <int SB, int SQ, typename T>
 GenParams<SB, SQ, T> make_params(const double* A, const double* B, const Geometry& geom) {
   GenParams<SB, SQ, T> P{};
@@ -396,7 +550,56 @@ RunFn select_dtype(int dtype, int SB, int SQ) {
   return f;
 }
 
+template <int SB, int SQ, typename T>
+void run_vjp(const double* A, const double* B, const Cells& cells, const Geometry& geom,
+             const void* x, const void* ybar, double* kbar, cudaStream_t stream) {
+  using V = VjpShape<SB, SQ>;
+  auto P = make_params<SB, SQ, T>(A, B, geom);
+  P.x = static_cast<const T*>(x);
+  P.ids = cells.ids;
+  P.ncells = cells.ncells;
+  P.nx = cells.nx;
+  P.ny = cells.ny;
+  P.nz = cells.nz;
+  if (cells.ncells == 0) return;
+  const size_t smem = (size_t)V::EPB * V::SE * sizeof(T);
+  SF_CUDA_CHECK(cudaFuncSetAttribute(k_kappa_vjp<SB, SQ, T>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long blocks = (cells.ncells + V::EPB - 1) / V::EPB;
+  SF_REQUIRE(blocks < (1LL << 31), SF_ERR_ARG, "too many cells for one launch");
+  k_kappa_vjp<SB, SQ, T><<<(unsigned)blocks, V::THREADS, smem, stream>>>(
+      P, static_cast<const T*>(ybar), kbar);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+using VjpFn = void (*)(const double*, const double*, const Cells&, const Geometry&, const void*,
+                       const void*, double*, cudaStream_t);
+
+template <typename T>
+VjpFn select_vjp(int SB, int SQ) {
+#define SF_CASE(sb, sq) \
+  if (SB == sb && SQ == sq) return &run_vjp<sb, sq, T>;
+#define SF_ROW(sb) SF_CASE(sb, sb - 1) SF_CASE(sb, sb) SF_CASE(sb, sb + 1) SF_CASE(sb, sb + 2)
+  SF_ROW(2) SF_ROW(3) SF_ROW(4) SF_ROW(5) SF_ROW(6) SF_ROW(7) SF_ROW(8)
+  SF_CASE(9, 8) SF_CASE(9, 9) SF_CASE(9, 10)
+  SF_CASE(10, 9) SF_CASE(10, 10)
+#undef SF_ROW
+#undef SF_CASE
+  return nullptr;
+}
+
 }  // namespace
+
+void launch_kappa_vjp(int dtype, int SB, int SQ, const double* A, const double* B,
+                      const Cells& cells, const Geometry& geom, const void* x, const void* ybar,
+                      double* kbar, cudaStream_t stream) {
+  VjpFn f = nullptr;
+  if (dtype == SF_F64) f = select_vjp<double>(SB, SQ);
+  else if (dtype == SF_F32) f = select_vjp<float>(SB, SQ);
+  else throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
+  if (!f) throw Error(SF_ERR_UNSUPPORTED, "no adjoint kernel for this SB/SQ");
+  f(A, B, cells, geom, x, ybar, kbar, stream);
+}
 
 void launch_general_apply(int dtype, int SB, int SQ, const double* A, const double* B,
                           const Cells& cells, const Geometry& geom, const void* x, void* y,

@@ -62,6 +62,10 @@ void launch_general_apply(int dtype, int SB, int SQ, const double* A, const doub
                           cudaStream_t stream);
 void launch_general_diag(int dtype, int SB, int SQ, const double* A, const double* B,
                          const Cells& cells, const Geometry& geom, void* d, cudaStream_t stream);
+// kbar[cell][q] = (grad ybar)_q^T G_q (grad x)_q, G without kappa (FP64 output).
+void launch_kappa_vjp(int dtype, int SB, int SQ, const double* A, const double* B,
+                      const Cells& cells, const Geometry& geom, const void* x, const void* ybar,
+                      double* kbar, cudaStream_t stream);
 // Cell-local evaluation: x_cells/y_cells [cell][SB^3] in local order; t2l (device) maps
 // tensor position -> local dof.
 void launch_general_evaluate(int dtype, int SB, int SQ, const double* A, const double* B,

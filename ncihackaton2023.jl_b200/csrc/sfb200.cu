@@ -559,6 +559,32 @@ int sf_set_coefficient(sf_op* op, const double* kappa) {
   });
 }
 
+int sf_set_coefficient_device(sf_op* op, const double* kappa, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(kappa, SF_ERR_ARG, "null kappa (use sf_set_coefficient(op, NULL) to clear)");
+    SF_REQUIRE(op->cells.mesh != sf::MESH_NONE, SF_ERR_STATE, "set the mesh before kappa");
+    const size_t n = (size_t)op->cells.ncells * op->SQ * op->SQ * op->SQ;
+    if (!op->d_kappa) op->d_kappa = dalloc<double>(n);
+    SF_CUDA_CHECK(cudaMemcpyAsync(op->d_kappa, kappa, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                  static_cast<cudaStream_t>(stream)));
+    op->geom.kappa = op->d_kappa;
+    invalidate_caches(op);
+    update_cartesian(op);
+  });
+}
+
+int sf_kappa_vjp(sf_op* op, int dtype, const void* x, const void* ybar, double* kappa_bar,
+                 void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(x && ybar && kappa_bar, SF_ERR_ARG, "null x, ybar or kappa_bar");
+    sf::launch_kappa_vjp(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, x,
+                         ybar, kappa_bar, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int sf_apply(sf_op* op, int dtype, const void* x, void* y, void* stream) {
   if (!op) return SF_ERR_ARG;
   return guarded(op, [&] { apply_impl(op, dtype, x, y, static_cast<cudaStream_t>(stream)); });

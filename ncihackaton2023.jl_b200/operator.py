@@ -174,16 +174,38 @@ class LazyMatrix:
 
     # -- extras -----------------------------------------------------------
     def set_coefficient(self, kappa):
-        """kappa at every quadrature point, shape (ncells, SQ^3), or None."""
+        """kappa at every quadrature point, shape (ncells, SQ^3), or None. A float64
+        CUDA tensor is copied on the device; anything else is read on the host."""
         if kappa is None:
             check(lib.sf_set_coefficient(self._h, None), self._h, "sf_set_coefficient")
             self.kappa = None
+            return
+        if torch is not None and isinstance(kappa, torch.Tensor) and kappa.is_cuda:
+            if kappa.dtype != torch.float64 or tuple(kappa.shape) != (self.model.num_cells,
+                                                                     self.m.SQ[0] ** 3):
+                raise ValueError("kappa must be float64 with shape (ncells, SQ^3)")
+            k = kappa.contiguous()
+            check(lib.sf_set_coefficient_device(self._h, C.c_void_p(k.data_ptr()), _stream()),
+                  self._h, "sf_set_coefficient_device")
+            self.kappa = k
             return
         k = _f64(kappa)
         if k.shape != (self.model.num_cells, self.m.SQ[0] ** 3):
             raise ValueError("kappa must have shape (ncells, SQ^3)")
         check(lib.sf_set_coefficient(self._h, _ptr(k)), self._h, "sf_set_coefficient")
         self.kappa = k
+
+    def kappa_vjp(self, x, ybar):
+        """d(ybar . A(kappa) x)/d kappa at every quadrature point, (ncells, SQ^3) FP64:
+        (grad ybar)^T G (grad x) per point, recomputed by sum factorization."""
+        if x.dtype != ybar.dtype or x.numel() != self.n or ybar.numel() != self.n:
+            raise ValueError("x and ybar must have the operator's size and one dtype")
+        kb = torch.empty(self.model.num_cells, self.m.SQ[0] ** 3, dtype=torch.float64,
+                         device=x.device)
+        check(lib.sf_kappa_vjp(self._h, _dtype_code(x.dtype), C.c_void_p(x.contiguous().data_ptr()),
+                               C.c_void_p(ybar.contiguous().data_ptr()), C.c_void_p(kb.data_ptr()),
+                               _stream()), self._h, "sf_kappa_vjp")
+        return kb
 
     def diagonal(self, dtype=None):
         """diag(A) as a device tensor."""

@@ -489,6 +489,49 @@ def assembled_sparse(m: OracleMap, mesh: OracleMesh, cq=None, kappa=None):
 
 
 # ----------------------------------------------------------------------------
+# Adjoint form: derivative of ybar . A(kappa) x with respect to kappa
+# ----------------------------------------------------------------------------
+
+
+def kappa_vjp(m: OracleMap, mesh: OracleMesh, x: np.ndarray, ybar: np.ndarray, cq=None,
+              chunk: int = 32768) -> np.ndarray:
+    """kappa_bar[c, q] = d(ybar . A(kappa) x)/d kappa_q
+    = wq djq sum_{r,k} (sum_l jq[l,r] jq[l,k]) (grad ybar)_r (grad x)_k, with the
+    reference gradients at the points from the restated ``_sumfac_dof2quad!``
+    (src/SumFactorizationKernels.jl:40-65) and the metric of
+    ``_sumfac_apply_weights!`` (:174-216). Returns (ncells, SQ^D)."""
+    if cq is None:
+        cq = cell_quantities(m, mesh)
+    wq, jq, djq = cq
+    D, SQ = m.D, m.SQ
+    xe, ye = gather(mesh, x), gather(mesh, ybar)
+    nc = xe.shape[0]
+    out = np.empty((nc, SQ ** D))
+    for s in range(0, nc, chunk):
+        e = min(nc, s + chunk)
+        gx = dof2quad(m, array2tensor(m, xe[s:e])).reshape(e - s, D, SQ ** D)
+        gy = dof2quad(m, array2tensor(m, ye[s:e])).reshape(e - s, D, SQ ** D)
+        C = np.einsum("cqlr,cqlk->cqrk", jq[s:e], jq[s:e])
+        out[s:e] = np.einsum("crq,cqrk,ckq->cq", gy, C, gx) * wq[s:e] * djq[s:e]
+    return out
+
+
+def adjoint_gradient_sparse(m: OracleMap, mesh: OracleMesh, b: np.ndarray, u_obs: np.ndarray,
+                            kappa: np.ndarray, cq=None):
+    """J(kappa) = 0.5 ||u - u_obs||^2 with A(kappa) u = b (sparse direct solves), and
+    dJ/dkappa = -kappa_vjp(u, lambda) with A lambda = u - u_obs. Returns (J, grad, u)."""
+    import scipy.sparse.linalg as spla
+    if cq is None:
+        cq = cell_quantities(m, mesh)
+    A = assembled_sparse(m, mesh, cq, kappa).tocsc()
+    lu = spla.splu(A)
+    u = lu.solve(b)
+    r = u - u_obs
+    lam = lu.solve(r)
+    return 0.5 * float(r @ r), -kappa_vjp(m, mesh, u, lam, cq), u
+
+
+# ----------------------------------------------------------------------------
 # Right-hand side, manufactured solution, Jacobi diagonal
 # ----------------------------------------------------------------------------
 

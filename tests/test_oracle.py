@@ -209,3 +209,40 @@ def test_manufactured_solution_converges():
         X = O.free_dof_coordinates(mesh)
         errs.append(np.abs(x - O.sin_solution(X)).max())
     assert errs[1] < errs[0] / 6.0
+
+
+def test_kappa_vjp_is_the_derivative():
+    """ybar . A(kappa) x is linear in kappa, so the VJP is exact: for any
+    direction d, ybar . (A(kappa + d) - A(kappa)) x = kappa_bar . d."""
+    m = O.make_map(3, 2, 4)
+    mesh = O.cartesian_mesh(3, 3, 2, m, perturb=0.15, seed=2)
+    cq = O.cell_quantities(m, mesh)
+    rng = np.random.default_rng(0)
+    nq = m.SQ ** 3
+    nc = mesh.cell_dof_ids.shape[0]
+    kappa = np.exp(rng.normal(0, 0.5, (nc, nq)))
+    d = rng.normal(0, 1, (nc, nq))
+    x = rng.uniform(-1, 1, mesh.n_free)
+    yb = rng.uniform(-1, 1, mesh.n_free)
+    kb = O.kappa_vjp(m, mesh, x, yb, cq)
+    lhs = yb @ (O.lazy_mul(m, mesh, x, cq, kappa + d) - O.lazy_mul(m, mesh, x, cq, kappa))
+    assert abs(lhs - np.sum(kb * d)) < 1e-12 * abs(lhs)
+
+
+def test_adjoint_gradient_matches_finite_differences():
+    m = O.make_map(3, 2, 4)
+    mesh = O.cartesian_mesh(3, 3, 2, m)
+    cq = O.cell_quantities(m, mesh)
+    rng = np.random.default_rng(1)
+    nc, nq = mesh.cell_dof_ids.shape[0], m.SQ ** 3
+    kappa = np.exp(rng.normal(0, 0.5, (nc, nq)))
+    kappa_true = np.exp(rng.normal(0, 0.5, (nc, nq)))
+    b = O.rhs(m, mesh, O.sin_forcing, cq)
+    _, _, u_obs = O.adjoint_gradient_sparse(m, mesh, b, np.zeros(mesh.n_free), kappa_true, cq)
+    J, g, _ = O.adjoint_gradient_sparse(m, mesh, b, u_obs, kappa, cq)
+    d = rng.normal(0, 1, (nc, nq))
+    eps = 1e-6
+    Jp = O.adjoint_gradient_sparse(m, mesh, b, u_obs, kappa + eps * d, cq)[0]
+    Jm = O.adjoint_gradient_sparse(m, mesh, b, u_obs, kappa - eps * d, cq)[0]
+    fd = (Jp - Jm) / (2 * eps)
+    assert abs(fd - np.sum(g * d)) < 1e-6 * abs(fd)
