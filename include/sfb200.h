@@ -202,6 +202,30 @@ int sf_autotune(sf_op* op, int dtype, void* stream);
 const char* sf_kernel_name(const sf_op* op, int dtype);
 
 /*
+ * Batched form: many independent Cartesian problems (handles on which the
+ * tiled kernel is in use), each with nrhs right-hand sides, applied by ONE
+ * CUDA-graph launch. Problems that share an order and 1D operators form a
+ * group. Each group is one persistent kernel whose CTAs take (problem,
+ * right-hand side, tile) work items from an atomic counter, and the groups
+ * run as concurrent branches of the graph. The reference has no batched form;
+ * it launched its CUDA.jl kernels one problem at a time (test/GPU_v3.jl:79-84).
+ *
+ * x[i], y[i]: device pointers to problem i's column-major (n_free_i x nrhs)
+ * blocks. The graph is captured on the first apply and re-captured when
+ * the pointers change. The handles must outlive the batch.
+ */
+typedef struct sf_batch sf_batch;
+int sf_batch_create(sf_batch** out, int nops, sf_op* const* ops, int nrhs);
+int sf_batch_destroy(sf_batch* b);
+const char* sf_batch_last_error(const sf_batch* b);
+int sf_batch_groups(const sf_batch* b, int* ngroups);
+int sf_batch_apply(sf_batch* b, int dtype, const void* const* x, void* const* y, void* stream);
+/* Pick the tile shape of every group by timing the candidates on x, y. */
+int sf_batch_autotune(sf_batch* b, int dtype, const void* const* x, void* const* y, void* stream);
+/* Tile shape used by a group for dtype (static string). */
+const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int group);
+
+/*
  * sf_cg_noalloc: sf_cg without any device or pinned-host allocation. It has no
  * counterpart in the reference.
  *

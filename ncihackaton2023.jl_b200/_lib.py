@@ -65,6 +65,13 @@ SIGNATURES = {
     "sf_autotune": (i32, [vp, i32, vp]),
     "sf_set_coefficient_device": (i32, [vp, vp, vp]),
     "sf_kappa_vjp": (i32, [vp, i32, vp, vp, vp, vp]),
+    "sf_batch_create": (i32, [C.POINTER(vp), i32, C.POINTER(vp), i32]),
+    "sf_batch_destroy": (i32, [vp]),
+    "sf_batch_last_error": (C.c_char_p, [vp]),
+    "sf_batch_groups": (i32, [vp, C.POINTER(i32)]),
+    "sf_batch_apply": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), vp]),
+    "sf_batch_autotune": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), vp]),
+    "sf_batch_group_kernel": (C.c_char_p, [vp, i32, i32]),
     "sf_kernel_name": (C.c_char_p, [vp, i32]),
 }
 

@@ -52,21 +52,21 @@ def kappa_apply(A: LazyMatrix, x: torch.Tensor, kappa: torch.Tensor) -> torch.Te
 
 
 def objective_gradient(A: LazyMatrix, b: torch.Tensor, u_obs: torch.Tensor, kappa: torch.Tensor,
-                       reltol: float = 1e-12, mode: str = "jacobi"):
+                       reltol: float = 1e-12, mode: str = "jacobi", maxiter: int = 20000):
     """J(kappa) = 0.5 ||u - u_obs||^2 with A(kappa) u = b, and dJ/dkappa by the adjoint
     method. Returns (J, grad (ncells, SQ^3), u, info)."""
     A.set_coefficient(kappa)
-    u, i1 = cg(A, b, reltol=reltol, mode=mode)
+    u, i1 = cg(A, b, reltol=reltol, mode=mode, maxiter=maxiter)
     res = u - u_obs
     J = 0.5 * torch.dot(res, res).item()
-    lam, i2 = cg(A, res, reltol=reltol, mode=mode)
+    lam, i2 = cg(A, res, reltol=reltol, mode=mode, maxiter=maxiter)
     grad = -A.kappa_vjp(u, lam)
     return J, grad, u, {"forward_iters": i1["iters"], "adjoint_iters": i2["iters"]}
 
 
 def objective(A: LazyMatrix, b: torch.Tensor, u_obs: torch.Tensor, kappa: torch.Tensor,
-              reltol: float = 1e-12, mode: str = "jacobi") -> float:
+              reltol: float = 1e-12, mode: str = "jacobi", maxiter: int = 20000) -> float:
     A.set_coefficient(kappa)
-    u, _ = cg(A, b, reltol=reltol, mode=mode)
+    u, _ = cg(A, b, reltol=reltol, mode=mode, maxiter=maxiter)
     r = u - u_obs
     return 0.5 * torch.dot(r, r).item()

@@ -37,6 +37,7 @@
 #include "sf_cartesian.cuh"
 
 #include <cmath>
+#include <cstring>
 
 namespace sf {
 namespace {
@@ -224,33 +225,25 @@ __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body&
   for (int j = 0; j < NOUT; ++j) ln[j][(E * P - 1) * st] = fin(j, r[j] + carry[j]);
 }
 
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
+// One output tile: cells [tx*EX, (tx+1)*EX) x [ty*EY, ...) x [tz*EZ, ...) of a free grid
+// nfx x nfy x nfz. T1/T2: shared buffers of Tile::TS words each. Ends with the
+// outputs stored; the caller synchronises before reusing T1/T2.
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T>
+__device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
+                                          const EOMat<P, T>& Km, const T* __restrict__ X,
+                                          T* __restrict__ Y, int nfx, int nfy, int nfz, int tx,
+                                          int ty, int tz, T rz, T rx, T cy) {
   using G = Tile<P, EX, EY, EZ, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* T1 = reinterpret_cast<T*>(smem_raw);  // t1 -> a -> y   [OZ][BY][BX]
-  T* T2 = T1 + G::TS;                        // t2 -> s        [OZ][BY][BX]
-
-  EOMat<P, T> Mm, Km;
-  Mm.load(Q.Me, Q.Mo);
-  Km.load(Q.Ke, Q.Ko);
-
-  const int tile = blockIdx.x;
-  const int tx = tile % Q.ntx;
-  const int ty = (tile / Q.ntx) % Q.nty;
-  const int tz = tile / (Q.ntx * Q.nty);
   // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
   const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
-  const int nfx = Q.nfx, nfy = Q.nfy, nfz = Q.nfz;
   const long long pz = (long long)nfx * nfy;
 
   // ---- z pass: one z-line per thread, read from global memory ----
-  for (int l = threadIdx.x; l < G::PLANE; l += NT) {
+  for (int l = threadIdx.x; l < G::BX * G::BY; l += NT) {
     const int x = l % G::BX, y = l / G::BX;
     const int fx = fx0 + x, fy = fy0 + y;
     const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
-    const T* col = Q.x + (long long)fx + (long long)nfx * fy;
+    const T* col = X + (long long)fx + (long long)nfx * fy;
     T c[G::BZ];
 #pragma unroll
     for (int z = 0; z < G::BZ; ++z) {
@@ -272,13 +265,13 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
       if (k > 0) {
         T1[(k * P - 1) * G::PLANE + l] = am.at(0) + cm;
         const T v = ak.at(0) + ck;
-        T2[(k * P - 1) * G::PLANE + l] = ISO ? v : v * Q.rz;
+        T2[(k * P - 1) * G::PLANE + l] = ISO ? v : v * rz;
       }
 #pragma unroll
       for (int m = 1; m < P; ++m) {
         T1[(k * P + m - 1) * G::PLANE + l] = am.at(m);
         const T v = ak.at(m);
-        T2[(k * P + m - 1) * G::PLANE + l] = ISO ? v : v * Q.rz;
+        T2[(k * P + m - 1) * G::PLANE + l] = ISO ? v : v * rz;
       }
       cm = am.at(P);
       ck = ak.at(P);
@@ -290,7 +283,7 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
       const Split<P, T> s = split<P, T>(u);
       T1[(EZ * P - 1) * G::PLANE + l] = mac_row0<P, T>(Mm, s, cm);
       const T v = mac_row0<P, T>(Km, s, ck);
-      T2[(EZ * P - 1) * G::PLANE + l] = ISO ? v : v * Q.rz;
+      T2[(EZ * P - 1) * G::PLANE + l] = ISO ? v : v * rz;
     }
   }
   __syncthreads();
@@ -310,7 +303,7 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
           r[0] = mac_row0<P, T>(Mm, s[0], T(0));
           r[1] = mac_row0<P, T>(Mm, s[1], mac_row0<P, T>(Km, s[0], T(0)));
         },
-        [&](int j, T v) { return (ISO || j == 1) ? v : v * Q.rx; });
+        [&](int j, T v) { return (ISO || j == 1) ? v : v * rx; });
   }
   __syncthreads();
 
@@ -327,7 +320,7 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
         [&](const Split<P, T>(&s)[2], T(&r)[1]) {
           r[0] = mac_row0<P, T>(Mm, s[1], mac_row0<P, T>(Km, s[0], T(0)));
         },
-        [&](int, T v) { return v * Q.cy; });
+        [&](int, T v) { return v * cy; });
   }
   __syncthreads();
 
@@ -340,9 +333,25 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
     const int zo = r / G::OY;
     const int fx = ox0 + xo, fy = oy0 + yo, fz = oz0 + zo;
     if (fx < nfx && fy < nfy && fz < nfz)
-      Q.y[(long long)fx + (long long)nfx * (fy + (long long)nfy * fz)] =
+      Y[(long long)fx + (long long)nfx * (fy + (long long)nfy * fz)] =
           T1[zo * G::PLANE + yo * G::BX + xo];
   }
+}
+
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
+  using G = Tile<P, EX, EY, EZ, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* T1 = reinterpret_cast<T*>(smem_raw);  // t1 -> a -> y   [OZ][BY][BX]
+  T* T2 = T1 + G::TS;                        // t2 -> s        [OZ][BY][BX]
+  EOMat<P, T> Mm, Km;
+  Mm.load(Q.Me, Q.Mo);
+  Km.load(Q.Ke, Q.Ko);
+  const int tile = blockIdx.x;
+  cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz,
+                                       tile % Q.ntx, (tile / Q.ntx) % Q.nty,
+                                       tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy);
 }
 
 template <int P, typename T>
@@ -358,6 +367,95 @@ void fill_eo(const double* M, double scale, T* ue, T* uo) {
     }
   for (int i = 0; i < S::NO; ++i)
     for (int j = i; j < S::NO; ++j) uo[tri(i, j, S::NO)] = (T)(0.5 * (m(i, j) - m(i, P - j)));
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: one persistent kernel applies many problems of the same order
+// (and the same 1D operators). The work items are (problem, right-hand side,
+// tile), numbered problem by problem. Every CTA takes the next item from a
+// global counter with one atomicAdd, until the items run out. No CTA ever waits
+// for another. The counter is zeroed before each launch.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct BatchProblem {
+  const T* x;
+  T* y;
+  long long ldx, ldy;   // elements between consecutive right-hand sides
+  long long first;      // index of the problem's first work item
+  int nfx, nfy, nfz;    // free grid
+  int ntx, nty, ntz;    // tiles
+  T rz, rx, cy;
+};
+
+template <int P, typename T>
+struct BatchParams {
+  T Me[EO<P>::UE], Mo[EO<P>::UO];
+  T Ke[EO<P>::UE], Ko[EO<P>::UO];
+  const BatchProblem<T>* probs;
+  int nprob;
+  long long total;  // work items
+  unsigned long long* counter;
+};
+
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+k_cartesian_batch(const __grid_constant__ BatchParams<P, T> Q) {
+  using G = Tile<P, EX, EY, EZ, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ long long s_item;
+  T* T1 = reinterpret_cast<T*>(smem_raw);
+  T* T2 = T1 + G::TS;
+  EOMat<P, T> Mm, Km;
+  Mm.load(Q.Me, Q.Mo);
+  Km.load(Q.Ke, Q.Ko);
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(Q.counter, 1ull);
+    __syncthreads();
+    const long long item = s_item;
+    if (item >= Q.total) break;  // the same value in every thread of the CTA
+    int lo = 0, hi = Q.nprob - 1;  // last problem whose first item <= item
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (Q.probs[mid].first <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchProblem<T> pb = Q.probs[lo];
+    const long long tiles = (long long)pb.ntx * pb.nty * pb.ntz;
+    const long long local = item - pb.first;
+    const long long rhs = local / tiles;
+    const int tile = (int)(local - rhs * tiles);
+    cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, pb.x + rhs * pb.ldx, pb.y + rhs * pb.ldy,
+                                         pb.nfx, pb.nfy, pb.nfz, tile % pb.ntx,
+                                         (tile / pb.ntx) % pb.nty, tile / (pb.ntx * pb.nty),
+                                         pb.rz, pb.rx, pb.cy);
+    __syncthreads();  // T1/T2 and s_item are reused by the next item
+  }
+}
+
+template <int P, typename T, int EX, int EY, int EZ, int NT, int MINB>
+void run_batch(const CartesianPlan& proto, const void* d_probs, int nprob, long long total,
+               unsigned long long* counter, bool iso, cudaStream_t st) {
+  using G = Tile<P, EX, EY, EZ, T>;
+  BatchParams<P, T> Q{};
+  fill_eo<P, T>(proto.M, 1.0, Q.Me, Q.Mo);
+  fill_eo<P, T>(proto.K, 1.0, Q.Ke, Q.Ko);
+  Q.probs = static_cast<const BatchProblem<T>*>(d_probs);
+  Q.nprob = nprob;
+  Q.total = total;
+  Q.counter = counter;
+  if (total == 0 || nprob == 0) return;
+  const size_t smem = (size_t)G::WORDS * sizeof(T);
+  auto kern = iso ? k_cartesian_batch<P, EX, EY, EZ, NT, true, T, MINB>
+                  : k_cartesian_batch<P, EX, EY, EZ, NT, false, T, MINB>;
+  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  SF_CUDA_CHECK(cudaGetDevice(&dev));
+  SF_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+  long long grid = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  if (grid > total) grid = total;
+  kern<<<(unsigned)grid, NT, smem, st>>>(Q);
+  SF_CUDA_CHECK(cudaGetLastError());
 }
 
 // One launch of the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
@@ -396,12 +494,17 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st
 }
 
 using RunFn = void (*)(const CartesianPlan&, const void*, void*, cudaStream_t);
+using BatchFn = void (*)(const CartesianPlan&, const void*, int, long long, unsigned long long*,
+                         bool, cudaStream_t);
 struct Candidate {
   RunFn run;
+  BatchFn batch;
+  int ex, ey, ez;
   const char* name;
 };
-#define SF_TILE(P_, T_, EX_, EY_, EZ_, NT_, MINB_) \
-  {&run_tile<P_, T_, EX_, EY_, EZ_, NT_, MINB_>, #EX_ "x" #EY_ "x" #EZ_ " cells, " #NT_ " thr, " #MINB_ "/SM"}
+#define SF_TILE(P_, T_, EX_, EY_, EZ_, NT_, MINB_)                                          \
+  {&run_tile<P_, T_, EX_, EY_, EZ_, NT_, MINB_>, &run_batch<P_, T_, EX_, EY_, EZ_, NT_, MINB_>, \
+   EX_, EY_, EZ_, #EX_ "x" #EY_ "x" #EZ_ " cells, " #NT_ " thr, " #MINB_ "/SM"}
 
 // Candidate tile shapes per (P, dtype); the first is the default. Shared
 // memory per CTA is 2 * PLANE * EZ*P words. The autotuner times them all on
@@ -549,5 +652,49 @@ void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* 
 }
 
 void cartesian_release(CartesianPlan& plan) { plan.ready = false; }
+
+size_t cartesian_batch_desc_bytes(int dtype) {
+  return dtype_slot(dtype) == 0 ? sizeof(BatchProblem<double>) : sizeof(BatchProblem<float>);
+}
+
+namespace {
+template <typename T>
+long long batch_desc(const CartesianPlan& plan, const Candidate& c, const void* x, void* y,
+                     long long ldx, long long ldy, int nrhs, long long first, void* out) {
+  BatchProblem<T> d{};
+  const int P = plan.SB - 1;
+  d.x = static_cast<const T*>(x);
+  d.y = static_cast<T*>(y);
+  d.ldx = ldx;
+  d.ldy = ldy;
+  d.first = first;
+  d.nfx = plan.nx * P - 1;
+  d.nfy = plan.ny * P - 1;
+  d.nfz = plan.nz * P - 1;
+  d.ntx = (plan.nx + c.ex - 1) / c.ex;
+  d.nty = (plan.ny + c.ey - 1) / c.ey;
+  d.ntz = (plan.nz + c.ez - 1) / c.ez;
+  d.rz = (T)(plan.c[2] / plan.c[1]);
+  d.rx = (T)(plan.c[0] / plan.c[1]);
+  d.cy = (T)plan.c[1];
+  std::memcpy(out, &d, sizeof(d));
+  return (long long)d.ntx * d.nty * d.ntz * nrhs;
+}
+}  // namespace
+
+long long cartesian_batch_desc(const CartesianPlan& plan, int dtype, int cand, const void* x,
+                               void* y, long long ldx, long long ldy, int nrhs, long long first,
+                               void* out) {
+  const Candidate& c = pick(plan, dtype, cand);
+  return dtype_slot(dtype) == 0 ? batch_desc<double>(plan, c, x, y, ldx, ldy, nrhs, first, out)
+                                : batch_desc<float>(plan, c, x, y, ldx, ldy, nrhs, first, out);
+}
+
+void cartesian_batch_launch(const CartesianPlan& proto, int dtype, int cand, const void* d_desc,
+                            int nprob, long long total, unsigned long long* d_counter, bool iso,
+                            cudaStream_t st) {
+  SF_REQUIRE(proto.ready, SF_ERR_STATE, "Cartesian plan not prepared");
+  pick(proto, dtype, cand).batch(proto, d_desc, nprob, total, d_counter, iso, st);
+}
 
 }  // namespace sf

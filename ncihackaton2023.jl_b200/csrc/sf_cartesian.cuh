@@ -25,6 +25,19 @@ const char* cartesian_candidate_name(const CartesianPlan& plan, int dtype, int k
 void cartesian_apply_candidate(const CartesianPlan& plan, int dtype, int k, const void* x, void* y,
                                cudaStream_t stream);
 int cartesian_launches(const CartesianPlan& plan);  // kernel launches per apply
+
+// Batched (persistent) form. A problem descriptor of cartesian_batch_desc_bytes(dtype)
+// bytes is written per problem; the call returns the problem's work items
+// (tiles of candidate `cand` x nrhs). One launch then applies every problem
+// of a group that shares `proto`'s order and 1D operators, with CTAs taking
+// work items from *d_counter (which must be zero at launch).
+size_t cartesian_batch_desc_bytes(int dtype);
+long long cartesian_batch_desc(const CartesianPlan& plan, int dtype, int cand, const void* x,
+                               void* y, long long ldx, long long ldy, int nrhs, long long first,
+                               void* out);
+void cartesian_batch_launch(const CartesianPlan& proto, int dtype, int cand, const void* d_desc,
+                            int nprob, long long total, unsigned long long* d_counter, bool iso,
+                            cudaStream_t st);
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
                      cudaStream_t stream);
 void cartesian_release(CartesianPlan& plan);

@@ -905,3 +905,297 @@ extern "C" int sf_cg_noalloc(sf_op* op, int mode, const double* b, double* x, do
     if (!(rel <= reltol)) throw Error(SF_ERR_NOT_CONVERGED, "CG reached its iteration cap");
   });
 }
+
+// ---------------------------------------------------------------------------
+// Batched form: many independent Cartesian problems, several right-hand
+// sides each, applied by one CUDA-graph launch. Problems are grouped by
+// order and 1D operators. Each group runs one persistent kernel over all its
+// (problem, right-hand side, tile) work items, and the groups are concurrent
+// branches of the graph.
+// ---------------------------------------------------------------------------
+struct sf_batch {
+  std::vector<sf_op*> ops;
+  int nrhs = 1;
+  struct Group {
+    std::vector<int> members;
+    bool iso = true;
+    int cand[2] = {0, 0};
+  };
+  std::vector<Group> groups;
+  struct PerDtype {
+    std::vector<const void*> xs;
+    std::vector<void*> ys;
+    char* d_desc = nullptr;                // descriptors of all groups, back to back
+    std::vector<size_t> desc_off;          // byte offset per group
+    std::vector<long long> total;          // work items per group
+    unsigned long long* d_counter = nullptr;  // one counter per group
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool dirty = true;
+  } st[2];
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev;
+  cudaStream_t cap = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int bfail(sf_batch* b, int status, const std::string& msg) {
+  if (b) b->err = msg;
+  return status;
+}
+
+template <typename F>
+int bguarded(sf_batch* b, F&& f) {
+  try {
+    f();
+    if (b) b->err.clear();
+    return SF_OK;
+  } catch (const Error& e) {
+    return bfail(b, e.status, e.what());
+  } catch (const std::exception& e) {
+    return bfail(b, SF_ERR_ARG, e.what());
+  }
+}
+
+void batch_free_dtype(sf_batch::PerDtype& s) {
+  if (s.exec) cudaGraphExecDestroy(s.exec);
+  if (s.graph) cudaGraphDestroy(s.graph);
+  dfree(s.d_desc);
+  dfree(s.d_counter);
+  s.exec = nullptr;
+  s.graph = nullptr;
+  s.d_desc = nullptr;
+  s.d_counter = nullptr;
+  s.dirty = true;
+}
+
+// (Re)write the descriptors of every group for the current vectors and candidates.
+void batch_descriptors(sf_batch* b, int slot, int dtype) {
+  auto& s = b->st[slot];
+  const size_t db = sf::cartesian_batch_desc_bytes(dtype);
+  std::vector<char> host;
+  s.desc_off.assign(b->groups.size(), 0);
+  s.total.assign(b->groups.size(), 0);
+  for (size_t g = 0; g < b->groups.size(); ++g) {
+    const auto& grp = b->groups[g];
+    s.desc_off[g] = host.size();
+    long long first = 0;
+    for (int i : grp.members) {
+      sf_op* op = b->ops[i];
+      const size_t at = host.size();
+      host.resize(at + db);
+      first += sf::cartesian_batch_desc(op->cart, dtype, grp.cand[slot], s.xs[i], s.ys[i],
+                                        op->n_free, op->n_free, b->nrhs, first, host.data() + at);
+    }
+    s.total[g] = first;
+  }
+  if (!s.d_desc) {
+    s.d_desc = dalloc<char>(host.size());
+    s.d_counter = dalloc<unsigned long long>(b->groups.size());
+  }
+  SF_CUDA_CHECK(cudaMemcpy(s.d_desc, host.data(), host.size(), cudaMemcpyHostToDevice));
+}
+
+void batch_launch_group(sf_batch* b, int slot, int dtype, size_t g, cudaStream_t st) {
+  auto& s = b->st[slot];
+  const auto& grp = b->groups[g];
+  sf::cartesian_batch_launch(b->ops[grp.members[0]]->cart, dtype, grp.cand[slot],
+                             s.d_desc + s.desc_off[g], (int)grp.members.size(), s.total[g],
+                             s.d_counter + g, grp.iso, st);
+}
+
+// Capture: zero the counters, then one persistent kernel per group on its own branch.
+void batch_capture(sf_batch* b, int slot, int dtype) {
+  auto& s = b->st[slot];
+  if (s.exec) cudaGraphExecDestroy(s.exec);
+  if (s.graph) cudaGraphDestroy(s.graph);
+  s.exec = nullptr;
+  s.graph = nullptr;
+  const size_t ng = b->groups.size();
+  while (b->side.size() < ng) {
+    cudaStream_t t;
+    SF_CUDA_CHECK(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+    b->side.push_back(t);
+  }
+  while (b->ev.size() < ng + 1) {
+    cudaEvent_t e;
+    SF_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ev.push_back(e);
+  }
+  if (!b->cap) SF_CUDA_CHECK(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  SF_CUDA_CHECK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+  try {
+    SF_CUDA_CHECK(cudaMemsetAsync(s.d_counter, 0, ng * sizeof(unsigned long long), b->cap));
+    SF_CUDA_CHECK(cudaEventRecord(b->ev[ng], b->cap));
+    for (size_t g = 0; g < ng; ++g) {
+      SF_CUDA_CHECK(cudaStreamWaitEvent(b->side[g], b->ev[ng], 0));
+      batch_launch_group(b, slot, dtype, g, b->side[g]);
+      SF_CUDA_CHECK(cudaEventRecord(b->ev[g], b->side[g]));
+      SF_CUDA_CHECK(cudaStreamWaitEvent(b->cap, b->ev[g], 0));
+    }
+  } catch (...) {
+    cudaGraph_t junk = nullptr;
+    cudaStreamEndCapture(b->cap, &junk);
+    if (junk) cudaGraphDestroy(junk);
+    throw;
+  }
+  SF_CUDA_CHECK(cudaStreamEndCapture(b->cap, &s.graph));
+  SF_CUDA_CHECK(cudaGraphInstantiate(&s.exec, s.graph, 0));
+  s.dirty = false;
+}
+
+int batch_slot(int dtype) {
+  if (dtype == SF_F64) return 0;
+  if (dtype == SF_F32) return 1;
+  throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
+}
+
+void batch_bind(sf_batch* b, int slot, const void* const* x, void* const* y) {
+  auto& s = b->st[slot];
+  const size_t n = b->ops.size();
+  bool changed = s.xs.size() != n;
+  if (!changed)
+    for (size_t i = 0; i < n; ++i)
+      if (s.xs[i] != x[i] || s.ys[i] != y[i]) changed = true;
+  if (changed) {
+    for (size_t i = 0; i < n; ++i)
+      SF_REQUIRE(x[i] && y[i] && x[i] != y[i], SF_ERR_ARG, "null or aliased x/y in the batch");
+    s.xs.assign(x, x + n);
+    s.ys.assign(y, y + n);
+    s.dirty = true;
+  }
+}
+
+}  // namespace
+
+extern "C" int sf_batch_create(sf_batch** out, int nops, sf_op* const* ops, int nrhs) {
+  if (!out || nops <= 0 || !ops || nrhs <= 0) return SF_ERR_ARG;
+  *out = nullptr;
+  sf_batch* b = new (std::nothrow) sf_batch();
+  if (!b) return SF_ERR_ARG;
+  int st = bguarded(b, [&] {
+    b->nrhs = nrhs;
+    b->ops.assign(ops, ops + nops);
+    for (int i = 0; i < nops; ++i) {
+      sf_op* op = b->ops[i];
+      SF_REQUIRE(op, SF_ERR_ARG, "null handle in the batch");
+      require_ready(op);
+      SF_REQUIRE(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64), SF_ERR_UNSUPPORTED,
+                 "batch member " + std::to_string(i) +
+                     " is not a constant-coefficient Cartesian problem (tiled kernel)");
+      // group by identical 1D operators (same order and quadrature)
+      size_t g = 0;
+      for (; g < b->groups.size(); ++g) {
+        const sf_op* r = b->ops[b->groups[g].members[0]];
+        if (r->SB == op->SB &&
+            std::memcmp(r->cart.M, op->cart.M, sizeof(op->cart.M)) == 0 &&
+            std::memcmp(r->cart.K, op->cart.K, sizeof(op->cart.K)) == 0)
+          break;
+      }
+      if (g == b->groups.size()) b->groups.emplace_back();
+      b->groups[g].members.push_back(i);
+      const double* c = op->cart.c;
+      if (!(c[0] == c[1] && c[1] == c[2])) b->groups[g].iso = false;
+    }
+  });
+  if (st != SF_OK) {
+    delete b;
+    return st;
+  }
+  *out = b;
+  return SF_OK;
+}
+
+extern "C" int sf_batch_destroy(sf_batch* b) {
+  if (!b) return SF_OK;
+  for (auto& s : b->st) batch_free_dtype(s);
+  for (auto t : b->side) cudaStreamDestroy(t);
+  for (auto e : b->ev) cudaEventDestroy(e);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  delete b;
+  return SF_OK;
+}
+
+extern "C" const char* sf_batch_last_error(const sf_batch* b) {
+  return b ? b->err.c_str() : "null batch";
+}
+
+extern "C" int sf_batch_groups(const sf_batch* b, int* ngroups) {
+  if (!b || !ngroups) return SF_ERR_ARG;
+  *ngroups = (int)b->groups.size();
+  return SF_OK;
+}
+
+extern "C" int sf_batch_apply(sf_batch* b, int dtype, const void* const* x, void* const* y,
+                              void* stream) {
+  if (!b || !x || !y) return SF_ERR_ARG;
+  return bguarded(b, [&] {
+    const int slot = batch_slot(dtype);
+    auto& s = b->st[slot];
+    batch_bind(b, slot, x, y);
+    if (s.dirty) {
+      batch_descriptors(b, slot, dtype);
+      batch_capture(b, slot, dtype);
+    }
+    SF_CUDA_CHECK(cudaGraphLaunch(s.exec, static_cast<cudaStream_t>(stream)));
+  });
+}
+
+extern "C" int sf_batch_autotune(sf_batch* b, int dtype, const void* const* x, void* const* y,
+                                 void* stream) {
+  if (!b || !x || !y) return SF_ERR_ARG;
+  return bguarded(b, [&] {
+    const int slot = batch_slot(dtype);
+    auto& s = b->st[slot];
+    batch_bind(b, slot, x, y);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SF_CUDA_CHECK(cudaEventCreate(&e0));
+    SF_CUDA_CHECK(cudaEventCreate(&e1));
+    try {
+      for (size_t g = 0; g < b->groups.size(); ++g) {
+        auto& grp = b->groups[g];
+        const int nc = sf::cartesian_candidates(b->ops[grp.members[0]]->cart, dtype);
+        int best = 0;
+        float best_ms = 0.f;
+        for (int k = 0; k < nc; ++k) {
+          grp.cand[slot] = k;
+          batch_descriptors(b, slot, dtype);
+          float ms = 0.f;
+          for (int rep = 0; rep < 3; ++rep) {  // first run warms up
+            SF_CUDA_CHECK(cudaMemsetAsync(s.d_counter + g, 0, sizeof(unsigned long long), st));
+            SF_CUDA_CHECK(cudaEventRecord(e0, st));
+            batch_launch_group(b, slot, dtype, g, st);
+            SF_CUDA_CHECK(cudaEventRecord(e1, st));
+            SF_CUDA_CHECK(cudaEventSynchronize(e1));
+            float t = 0.f;
+            SF_CUDA_CHECK(cudaEventElapsedTime(&t, e0, e1));
+            if (rep > 0) ms += t;
+          }
+          if (k == 0 || ms < best_ms) {
+            best = k;
+            best_ms = ms;
+          }
+        }
+        grp.cand[slot] = best;
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s.dirty = true;  // descriptors and graph follow the chosen candidates
+  });
+}
+
+extern "C" const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int group) {
+  if (!b || group < 0 || group >= (int)b->groups.size()) return "invalid group";
+  if (dtype != SF_F64 && dtype != SF_F32) return "invalid dtype";
+  const auto& grp = b->groups[group];
+  return sf::cartesian_candidate_name(b->ops[grp.members[0]]->cart, dtype,
+                                      grp.cand[dtype == SF_F64 ? 0 : 1]);
+}

@@ -68,3 +68,16 @@ def test_zero_rhs(sf):
     A, V, om, mesh, b, bd = setup(sf, 2, 4, 3)
     x, info = sf.cg(A, torch.zeros_like(bd), reltol=1e-10)
     assert info["iters"] == 0 and x.abs().max().item() == 0.0
+
+
+def test_deformed_q8_iterations_match_oracle(sf):
+    """High-order deformed cells (equispaced Q8, kappa(A) large): the device
+    Jacobi CG follows the oracle's iteration count."""
+    A, V, om, mesh, b, bd = setup(sf, 8, 16, 2, perturb=0.2)
+    S = O.assembled_sparse(om, mesh)
+    d = S.diagonal()
+    x_ref, it_ref, _ = O.cg(lambda v: S @ v, b, reltol=1e-10, precond=lambda r: r / d,
+                            maxiter=20000)
+    x, info = sf.cg(A, bd, reltol=1e-10, mode="jacobi", maxiter=20000)
+    assert info["converged"] and abs(info["iters"] - it_ref) <= max(2, it_ref // 50)
+    assert np.abs(x.cpu().numpy() - x_ref).max() < 1e-7 * np.abs(x_ref).max()
