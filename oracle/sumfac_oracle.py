@@ -469,7 +469,12 @@ def element_matrices(m: OracleMap, cq, kappa=None) -> np.ndarray:
     s = wq * djq
     if kappa is not None:
         s = s * kappa
-    return np.einsum("cq,cqal,cqbl->cab", s, P, P)
+    nc, nq, na, _ = P.shape
+    Ke = np.empty((nc, na, na))
+    for c in range(nc):  # K_e = sum_q s_q P_q P_q^T as one BLAS product per cell
+        Pc = P[c].transpose(1, 0, 2).reshape(na, nq * D)
+        Ke[c] = (Pc * np.repeat(s[c], D)[None, :]) @ Pc.T
+    return Ke
 
 
 def assembled_sparse(m: OracleMap, mesh: OracleMesh, cq=None, kappa=None):
