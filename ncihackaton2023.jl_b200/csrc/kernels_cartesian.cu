@@ -183,17 +183,21 @@ template <int P, int E, int NIN, int NOUT, typename T, typename Body, typename R
 __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body& body,
                                           const Row0& row0, const Fin& fin) {
   T u[NIN][P + 1];
+  T un[NIN][P];  // next cell's nodes 1..P, loaded while the current cell computes
   T carry[NOUT];
 #pragma unroll
   for (int j = 0; j < NOUT; ++j) carry[j] = T(0);
-#pragma unroll 1
+#pragma unroll
+  for (int i = 0; i < NIN; ++i)
+#pragma unroll
+    for (int l = 0; l <= P; ++l) u[i][l] = ln[i][l * st];
+#pragma unroll(sizeof(T) == 8 ? E : 1)  // FP64: unrolled, no register shuffles between cells
   for (int k = 0; k < E; ++k) {
+    // prefetch: cell k+1 reads (k+1)P+1..(k+1)P+P, above every index cell k writes
 #pragma unroll
-    for (int i = 0; i < NIN; ++i) {
+    for (int i = 0; i < NIN; ++i)
 #pragma unroll
-      for (int l = 0; l <= P; ++l)
-        if (k == 0 || l > 0) u[i][l] = ln[i][(k * P + l) * st];
-    }
+      for (int l = 1; l <= P; ++l) un[i][l - 1] = ln[i][((k + 1) * P + l) * st];
     Split<P, T> s[NIN];
 #pragma unroll
     for (int i = 0; i < NIN; ++i) s[i] = split<P, T>(u[i]);
@@ -209,13 +213,13 @@ __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body&
       carry[j] = acc[j].at(P);
     }
 #pragma unroll
-    for (int i = 0; i < NIN; ++i) u[i][0] = u[i][P];
+    for (int i = 0; i < NIN; ++i) {
+      u[i][0] = u[i][P];
+#pragma unroll
+      for (int l = 1; l <= P; ++l) u[i][l] = un[i][l - 1];
+    }
   }
-  // last cell: node 0 only (the end point E*P)
-#pragma unroll
-  for (int i = 0; i < NIN; ++i)
-#pragma unroll
-    for (int l = 1; l <= P; ++l) u[i][l] = ln[i][(E * P + l) * st];
+  // last cell: node 0 only (the end point E*P); its inputs are already in u
   Split<P, T> s[NIN];
 #pragma unroll
   for (int i = 0; i < NIN; ++i) s[i] = split<P, T>(u[i]);
@@ -238,18 +242,29 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
   const long long pz = (long long)nfx * nfy;
 
+  // a tile whose whole input box lies inside the free grid needs no bounds checks
+  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= 0 && fx0 + G::BX <= nfx &&
+                        fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
+
   // ---- z pass: one z-line per thread, read from global memory ----
-  for (int l = threadIdx.x; l < G::BX * G::BY; l += NT) {
+  auto load_col = [&](int l, T (&c)[G::BZ]) {
     const int x = l % G::BX, y = l / G::BX;
     const int fx = fx0 + x, fy = fy0 + y;
-    const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
-    const T* col = X + (long long)fx + (long long)nfx * fy;
-    T c[G::BZ];
+    if (interior) {
+      const T* col = X + (long long)fx + (long long)nfx * fy + fz0 * pz;
 #pragma unroll
-    for (int z = 0; z < G::BZ; ++z) {
-      const int fz = fz0 + z;
-      c[z] = (inxy && (unsigned)fz < (unsigned)nfz) ? col[fz * pz] : T(0);
+      for (int z = 0; z < G::BZ; ++z) c[z] = __ldg(col + z * pz);
+    } else {
+      const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
+      const T* col = X + (long long)fx + (long long)nfx * fy;
+#pragma unroll
+      for (int z = 0; z < G::BZ; ++z) {
+        const int fz = fz0 + z;
+        c[z] = (inxy && (unsigned)fz < (unsigned)nfz) ? __ldg(col + fz * pz) : T(0);
+      }
     }
+  };
+  auto z_line = [&](int l, const T (&c)[G::BZ]) {
     T cm = T(0), ck = T(0);
 #pragma unroll
     for (int k = 0; k < EZ; ++k) {
@@ -276,14 +291,28 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
       cm = am.at(P);
       ck = ak.at(P);
     }
-    {
-      T u[P + 1];
+    T u[P + 1];
 #pragma unroll
-      for (int m = 0; m <= P; ++m) u[m] = c[EZ * P + m];
-      const Split<P, T> s = split<P, T>(u);
-      T1[(EZ * P - 1) * G::PLANE + l] = mac_row0<P, T>(Mm, s, cm);
-      const T v = mac_row0<P, T>(Km, s, ck);
-      T2[(EZ * P - 1) * G::PLANE + l] = ISO ? v : v * rz;
+    for (int m = 0; m <= P; ++m) u[m] = c[EZ * P + m];
+    const Split<P, T> s = split<P, T>(u);
+    T1[(EZ * P - 1) * G::PLANE + l] = mac_row0<P, T>(Mm, s, cm);
+    const T v = mac_row0<P, T>(Km, s, ck);
+    T2[(EZ * P - 1) * G::PLANE + l] = ISO ? v : v * rz;
+  };
+  constexpr int ZL = G::BX * G::BY;
+  if constexpr (ZL > NT && ZL <= 2 * NT) {
+    // two z-lines per thread: both columns' loads are in flight before either computes
+    const int l0 = threadIdx.x, l1 = threadIdx.x + NT;
+    T c0[G::BZ], c1[G::BZ];
+    load_col(l0, c0);
+    if (l1 < ZL) load_col(l1, c1);
+    z_line(l0, c0);
+    if (l1 < ZL) z_line(l1, c1);
+  } else {
+    for (int l = threadIdx.x; l < ZL; l += NT) {
+      T c[G::BZ];
+      load_col(l, c);
+      z_line(l, c);
     }
   }
   __syncthreads();
@@ -326,15 +355,15 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
 
   // ---- store the owned outputs (free coords start at e0*p) ----
   const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
+  const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz;
+  T* ybase = Y + (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
   for (int i = threadIdx.x; i < G::OX * G::OY * G::OZ; i += NT) {
     const int xo = i % G::OX;
     const int r = i / G::OX;
     const int yo = r % G::OY;
     const int zo = r / G::OY;
-    const int fx = ox0 + xo, fy = oy0 + yo, fz = oz0 + zo;
-    if (fx < nfx && fy < nfy && fz < nfz)
-      Y[(long long)fx + (long long)nfx * (fy + (long long)nfy * fz)] =
-          T1[zo * G::PLANE + yo * G::BX + xo];
+    if (full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz))
+      ybase[xo + (long long)nfx * (yo + (long long)nfy * zo)] = T1[zo * G::PLANE + yo * G::BX + xo];
   }
 }
 
@@ -517,10 +546,13 @@ template <> struct Cands<2, double> { static constexpr Candidate c[] = {SF_TILE(
 template <> struct Cands<3, double> { static constexpr Candidate c[] = {SF_TILE(3, double, 4, 4, 2, 256, 2),
                                                                       SF_TILE(3, double, 4, 4, 3, 256, 2)}; };
 template <> struct Cands<4, double> { static constexpr Candidate c[] = {SF_TILE(4, double, 4, 4, 2, 256, 3),
+                                                                      SF_TILE(4, double, 4, 4, 2, 256, 2),
                                                                       SF_TILE(4, double, 4, 4, 3, 256, 2),
                                                                       SF_TILE(4, double, 4, 4, 4, 256, 2),
                                                                       SF_TILE(4, double, 4, 4, 2, 224, 3),
-                                                                      SF_TILE(4, double, 4, 4, 3, 320, 2)}; };
+                                                                      SF_TILE(4, double, 4, 4, 3, 320, 2),
+                                                                      SF_TILE(4, double, 4, 4, 1, 128, 6),
+                                                                      SF_TILE(4, double, 8, 4, 2, 256, 2)}; };
 template <> struct Cands<5, double> { static constexpr Candidate c[] = {SF_TILE(5, double, 2, 2, 2, 256, 2)}; };
 template <> struct Cands<6, double> { static constexpr Candidate c[] = {SF_TILE(6, double, 2, 2, 2, 256, 1)}; };
 template <> struct Cands<7, double> { static constexpr Candidate c[] = {SF_TILE(7, double, 2, 2, 1, 256, 1)}; };

@@ -13,9 +13,9 @@
 //   backward the transposes in reverse order.
 // Every pass gives each thread one full 1D line, read from shared memory into
 // registers. The thread computes all outputs of the line, so every value
-// loaded is reused SQ (or SB) times. The 1D matrices sit in the kernel's
-// __grid_constant__ parameters, so the FMAs take them straight from the
-// constant bank. The scatter-add uses atomics into a y that was zeroed before
+// loaded is reused SQ (or SB) times. The 1D matrices are passed in the kernel's
+// __grid_constant__ parameters (staged in shared memory for FP64 at high order,
+// see kStageMats). The scatter-add uses atomics into a y that was zeroed before
 // the launch. Dirichlet dofs (id < 0) read as zero and are skipped.
 #include "sf_internal.cuh"
 
@@ -71,6 +71,26 @@ __device__ __forceinline__ long long structured_index(long long c, int pos, int 
 template <typename T>
 __device__ __forceinline__ void atomic_add(T* a, T v) { atomicAdd(a, v); }
 
+// FP64 FMAs cannot take a 64-bit operand from the constant bank. At high
+// order (SQ*SB >= 64) the FP64 1D matrices are therefore staged once per CTA
+// in shared memory and read with broadcast loads; keeping 2*SQ*SB doubles in
+// registers would cost up to 162 registers per thread at Q8. At lower orders,
+// and in FP32, they are read straight from the kernel parameters.
+template <typename T, int SB, int SQ>
+constexpr bool kStageMats = sizeof(T) == 8 && SQ * SB >= 64;
+#define MA(i) (kStageMats<T, SB, SQ> ? sMat[(i)] : P.A[(i)])
+#define MB(i) (kStageMats<T, SB, SQ> ? sMat[SQ * SB + (i)] : P.B[(i)])
+
+template <int SB, int SQ, typename T>
+__device__ __forceinline__ void stage_mats(const GenParams<SB, SQ, T>& P, T* sMat) {
+  if constexpr (kStageMats<T, SB, SQ>) {
+    for (int i = threadIdx.x; i < SQ * SB; i += blockDim.x) {
+      sMat[i] = P.A[i];
+      sMat[SQ * SB + i] = P.B[i];
+    }
+  }
+}
+
 template <int SB, int SQ, typename T>
 __global__ void __launch_bounds__(Shape<SB, SQ>::THREADS)
 k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
@@ -87,6 +107,8 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   T* AA = B1 + S::S1;
   T* AB = AA + S::S2;
   T* BA = AB + S::S2;
+  __shared__ T sMat[kStageMats<T, SB, SQ> ? 2 * SQ * SB : 1];
+  stage_mats<SB, SQ, T>(P, sMat);  // visible after the first __syncthreads below
 
   // ---------------- gather ----------------
   for (int pos = l; pos < S::S0; pos += S::NL) {
@@ -118,8 +140,8 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       T a = T(0), b = T(0);
 #pragma unroll
       for (int i = 0; i < SB; ++i) {
-        a = fma(P.A[qi * SB + i], in[i], a);
-        b = fma(P.B[qi * SB + i], in[i], b);
+        a = fma(MA(qi * SB + i), in[i], a);
+        b = fma(MB(qi * SB + i), in[i], b);
       }
       A1[line * SQ + qi] = a;
       B1[line * SQ + qi] = b;
@@ -141,9 +163,9 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       T aa = T(0), ab = T(0), ba = T(0);
 #pragma unroll
       for (int j = 0; j < SB; ++j) {
-        aa = fma(P.A[qj * SB + j], a1[j], aa);
-        ab = fma(P.B[qj * SB + j], a1[j], ab);
-        ba = fma(P.A[qj * SB + j], b1[j], ba);
+        aa = fma(MA(qj * SB + j), a1[j], aa);
+        ab = fma(MB(qj * SB + j), a1[j], ab);
+        ba = fma(MA(qj * SB + j), b1[j], ba);
       }
       const int o = (k * SQ + qj) * SQ + qi;
       AA[o] = aa;
@@ -172,9 +194,9 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       T ux = T(0), uy = T(0), uz = T(0);
 #pragma unroll
       for (int k = 0; k < SB; ++k) {
-        ux = fma(P.A[qk * SB + k], ba[k], ux);
-        uy = fma(P.A[qk * SB + k], ab[k], uy);
-        uz = fma(P.B[qk * SB + k], aa[k], uz);
+        ux = fma(MA(qk * SB + k), ba[k], ux);
+        uy = fma(MA(qk * SB + k), ab[k], uy);
+        uz = fma(MB(qk * SB + k), aa[k], uz);
       }
       // metric in FP64 (geometric factors are kept in FP64 for both dtypes)
       const int q = qi + SQ * (qj + SQ * qk);
@@ -199,9 +221,9 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       const T vz = (T)(g[4] * dx + g[5] * dy + g[2] * dz);
 #pragma unroll
       for (int k = 0; k < SB; ++k) {
-        ba_o[k] = fma(P.A[qk * SB + k], vx, ba_o[k]);
-        ab_o[k] = fma(P.A[qk * SB + k], vy, ab_o[k]);
-        aa_o[k] = fma(P.B[qk * SB + k], vz, aa_o[k]);
+        ba_o[k] = fma(MA(qk * SB + k), vx, ba_o[k]);
+        ab_o[k] = fma(MA(qk * SB + k), vy, ab_o[k]);
+        aa_o[k] = fma(MB(qk * SB + k), vz, aa_o[k]);
       }
     }
 #pragma unroll
@@ -230,9 +252,9 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       T a1 = T(0), b1 = T(0);
 #pragma unroll
       for (int qj = 0; qj < SQ; ++qj) {
-        a1 = fma(P.A[qj * SB + j], aa[qj], a1);
-        a1 = fma(P.B[qj * SB + j], ab[qj], a1);
-        b1 = fma(P.A[qj * SB + j], ba[qj], b1);
+        a1 = fma(MA(qj * SB + j), aa[qj], a1);
+        a1 = fma(MB(qj * SB + j), ab[qj], a1);
+        b1 = fma(MA(qj * SB + j), ba[qj], b1);
       }
       A1[(k * SB + j) * SQ + qi] = a1;
       B1[(k * SB + j) * SQ + qi] = b1;
@@ -254,8 +276,8 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       T yv = T(0);
 #pragma unroll
       for (int qi = 0; qi < SQ; ++qi) {
-        yv = fma(P.A[qi * SB + i], a1[qi], yv);
-        yv = fma(P.B[qi * SB + i], b1[qi], yv);
+        yv = fma(MA(qi * SB + i), a1[qi], yv);
+        yv = fma(MB(qi * SB + i), b1[qi], yv);
       }
       X[line * SB + i] = yv;
     }
@@ -338,8 +360,8 @@ struct VjpShape {
 
 // forward passes x/y of the element kernel: X -> (A1, B1) -> (AA, AB, BA)
 template <int SB, int SQ, typename T>
-__device__ __forceinline__ void forward_xy(const GenParams<SB, SQ, T>& P, int l, const T* X, T* A1,
-                                           T* B1, T* AA, T* AB, T* BA) {
+__device__ __forceinline__ void forward_xy(const GenParams<SB, SQ, T>& P, const T* sMat, int l,
+                                           const T* X, T* A1, T* B1, T* AA, T* AB, T* BA) {
   if (l < SB * SB) {
     T in[SB];
 #pragma unroll
@@ -349,8 +371,8 @@ __device__ __forceinline__ void forward_xy(const GenParams<SB, SQ, T>& P, int l,
       T a = T(0), b = T(0);
 #pragma unroll
       for (int i = 0; i < SB; ++i) {
-        a = fma(P.A[qi * SB + i], in[i], a);
-        b = fma(P.B[qi * SB + i], in[i], b);
+        a = fma(MA(qi * SB + i), in[i], a);
+        b = fma(MB(qi * SB + i), in[i], b);
       }
       A1[l * SQ + qi] = a;
       B1[l * SQ + qi] = b;
@@ -370,9 +392,9 @@ __device__ __forceinline__ void forward_xy(const GenParams<SB, SQ, T>& P, int l,
       T aa = T(0), ab = T(0), ba = T(0);
 #pragma unroll
       for (int j = 0; j < SB; ++j) {
-        aa = fma(P.A[qj * SB + j], a1[j], aa);
-        ab = fma(P.B[qj * SB + j], a1[j], ab);
-        ba = fma(P.A[qj * SB + j], b1[j], ba);
+        aa = fma(MA(qj * SB + j), a1[j], aa);
+        ab = fma(MB(qj * SB + j), a1[j], ab);
+        ba = fma(MA(qj * SB + j), b1[j], ba);
       }
       const int o = (k * SQ + qj) * SQ + qi;
       AA[o] = aa;
@@ -405,6 +427,8 @@ k_kappa_vjp(const __grid_constant__ GenParams<SB, SQ, T> P, const T* __restrict_
     buf[v][4] = buf[v][3] + S::S2;        // AB
     buf[v][5] = buf[v][4] + S::S2;        // BA
   }
+  __shared__ T sMat[kStageMats<T, SB, SQ> ? 2 * SQ * SB : 1];
+  stage_mats<SB, SQ, T>(P, sMat);  // visible after the first __syncthreads below
   // gather x and ybar
   for (int pos = l; pos < S::S0; pos += S::NL) {
     T vx = T(0), vy = T(0);
@@ -421,8 +445,10 @@ k_kappa_vjp(const __grid_constant__ GenParams<SB, SQ, T> P, const T* __restrict_
     buf[1][0][pos] = vy;
   }
   __syncthreads();
-  forward_xy<SB, SQ, T>(P, l, buf[0][0], buf[0][1], buf[0][2], buf[0][3], buf[0][4], buf[0][5]);
-  forward_xy<SB, SQ, T>(P, l, buf[1][0], buf[1][1], buf[1][2], buf[1][3], buf[1][4], buf[1][5]);
+  forward_xy<SB, SQ, T>(P, sMat, l, buf[0][0], buf[0][1], buf[0][2], buf[0][3], buf[0][4],
+                        buf[0][5]);
+  forward_xy<SB, SQ, T>(P, sMat, l, buf[1][0], buf[1][1], buf[1][2], buf[1][3], buf[1][4],
+                        buf[1][5]);
   __syncthreads();
   if (l < SQ * SQ && valid) {
     const int qi = l % SQ, qj = l / SQ;
@@ -444,9 +470,9 @@ k_kappa_vjp(const __grid_constant__ GenParams<SB, SQ, T> P, const T* __restrict_
         T gx = T(0), gy = T(0), gz = T(0);
 #pragma unroll
         for (int k = 0; k < SB; ++k) {
-          gx = fma(P.A[qk * SB + k], c[v][0][k], gx);
-          gy = fma(P.A[qk * SB + k], c[v][1][k], gy);
-          gz = fma(P.B[qk * SB + k], c[v][2][k], gz);
+          gx = fma(MA(qk * SB + k), c[v][0][k], gx);
+          gy = fma(MA(qk * SB + k), c[v][1][k], gy);
+          gz = fma(MB(qk * SB + k), c[v][2][k], gz);
         }
         g[v][0] = (double)gx;
         g[v][1] = (double)gy;
