@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves")
+    ap.add_argument("--cg-only", action="store_true",
+                    help="only the CG solves (autotuned tiles; no apply leg): for profiling")
+    ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-secondary", action="store_true",
@@ -199,6 +202,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     m, model, V, A = build_problem(sf)
+    if args.cg_only:
+        A.autotune(torch.float64)
+        A.autotune(torch.float32)
+        return {"cg": run_cg(sf, m, model, V, A, dev, args.cg_maxiter)}
     tile_ms = {}
     if args.tile is not None:
         A.set_option("tile_candidate_f64", args.tile)
@@ -303,7 +310,7 @@ def run_ours(args, rank, world, local_rank):
                 out[key] = {"error": f"{type(e).__name__}: {e}"}
             log(f"{key}: {out[key]}")
     if not args.no_cg:
-        out["cg"] = run_cg(sf, m, model, V, A, dev)
+        out["cg"] = run_cg(sf, m, model, V, A, dev, args.cg_maxiter)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline_port()
     if world > 1:
@@ -315,23 +322,26 @@ CG_MAXITER = 6000
 SECONDARY_BUDGET_S = 180.0
 
 
-def _timed_solves(sf, A, b, u_exact=None, warm=True):
+def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
     import torch
     res, sols = {}, {}
     for mode in ("jacobi", "mixed"):
         if warm:  # workspaces, diagonal
-            sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=CG_MAXITER, raise_on_fail=False)
+            sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=maxiter, raise_on_fail=False)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        x, info = sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=CG_MAXITER, raise_on_fail=False)
-        e1.record()
-        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record()
+            x, info = sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=maxiter, raise_on_fail=False)
+            e1.record()
+            torch.cuda.synchronize()
         sols[mode] = x
         key = "f64" if mode == "jacobi" else "mixed"
-        res[key] = {"ms": round(e0.elapsed_time(e1), 3), "iters": info["iters"],
+        ms = e0.elapsed_time(e1)
+        res[key] = {"ms": round(ms, 3), "iters": info["iters"],
+                    "ms_per_iter": round(ms / max(1, info["iters"]), 4),
                     "refinements": info["outer"], "relres": info["relres"],
-                    "converged": info["converged"]}
+                    "converged": info["converged"], "clocks": clk.summary()}
         log(f"cg {key}: {res[key]}")
         if u_exact is not None:
             res[key]["err_vs_exact_max"] = (x - u_exact).abs().max().item()
@@ -341,7 +351,7 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True):
     return res
 
 
-def run_cg(sf, m, model, V, A, dev):
+def run_cg(sf, m, model, V, A, dev, maxiter=CG_MAXITER):
     """CG to relres 1e-10: the manufactured problem of the benchmark
     (f = 3 pi^2 sin sin sin), and a rough right-hand side (b ~ U[-1,1], seed
     1), both FP64 Jacobi CG and mixed precision (FP32 recurrence and apply,
@@ -351,10 +361,10 @@ def run_cg(sf, m, model, V, A, dev):
                                                                                axis=-1))).to(dev)
     X = V.free_dof_coordinates()
     u_exact = torch.from_numpy(np.prod(np.sin(np.pi * X), axis=1)).to(dev)
-    res = _timed_solves(sf, A, b, u_exact)
+    res = _timed_solves(sf, A, b, u_exact, maxiter=maxiter)
     res["preconditioner"] = "Jacobi (matrix-free diagonal)"
     b_rough = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, V.num_free_dofs)).to(dev)
-    res["rough_rhs"] = _timed_solves(sf, A, b_rough)
+    res["rough_rhs"] = _timed_solves(sf, A, b_rough, maxiter=maxiter)
     return res
 
 

@@ -67,7 +67,24 @@ struct CartParams {
   T* y;
   int nfx, nfy, nfz;  // free grid
   int ntx, nty, ntz;  // tiles
+  double* dot;  // non-null: dot[tile] = sum of x*y over the tile's outputs
 };
+
+// FP64 sum over the CTA, valid in thread 0 (adds warps in a fixed order).
+template <int NT>
+__device__ __forceinline__ double cta_sum(double v) {
+  __shared__ double red[NT / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) t += red[w];
+  }
+  return t;
+}
 
 // Even/odd parts of one operator, held in registers (symmetric entries share one register).
 template <int P, typename T>
@@ -231,12 +248,15 @@ __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body&
 
 // One output tile: cells [tx*EX, (tx+1)*EX) x [ty*EY, ...) x [tz*EZ, ...) of a free grid
 // nfx x nfy x nfz. T1/T2: shared buffers of Tile::TS words each. Ends with the
-// outputs stored; the caller synchronises before reusing T1/T2.
+// outputs stored; the caller synchronises before reusing T1/T2. With `dot`
+// non-null, *dot receives the FP64 sum of x*y over the tile's outputs (the
+// (p, A p) term of CG), summed in a fixed order.
 template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T>
 __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
                                           const EOMat<P, T>& Km, const T* __restrict__ X,
                                           T* __restrict__ Y, int nfx, int nfy, int nfz, int tx,
-                                          int ty, int tz, T rz, T rx, T cy) {
+                                          int ty, int tz, T rz, T rx, T cy,
+                                          double* dot = nullptr) {
   using G = Tile<P, EX, EY, EZ, T>;
   // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
   const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
@@ -356,15 +376,50 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   // ---- store the owned outputs (free coords start at e0*p) ----
   const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
   const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz;
-  T* ybase = Y + (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
-  for (int i = threadIdx.x; i < G::OX * G::OY * G::OZ; i += NT) {
+  const long long base = (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
+  T* ybase = Y + base;
+  constexpr int NOUT = G::OX * G::OY * G::OZ;
+  auto out_index = [&](int i, long long& o, int& t1) {  // false outside the free grid
     const int xo = i % G::OX;
     const int r = i / G::OX;
     const int yo = r % G::OY;
     const int zo = r / G::OY;
-    if (full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz))
-      ybase[xo + (long long)nfx * (yo + (long long)nfy * zo)] = T1[zo * G::PLANE + yo * G::BX + xo];
+    o = xo + (long long)nfx * (yo + (long long)nfy * zo);
+    t1 = zo * G::PLANE + yo * G::BX + xo;
+    return full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz);
+  };
+  if (!dot) {
+    for (int i = threadIdx.x; i < NOUT; i += NT) {
+      long long o;
+      int t1;
+      if (out_index(i, o, t1)) ybase[o] = T1[t1];
+    }
+    return;
   }
+  // with the (x, y) sum: every x value of this thread is requested before any is used
+  constexpr int PER = (NOUT + NT - 1) / NT;
+  T xv[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = threadIdx.x + k * NT;
+    long long o;
+    int t1;
+    xv[k] = (i < NOUT && out_index(i, o, t1)) ? __ldg(X + base + o) : T(0);
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int i = threadIdx.x + k * NT;
+    long long o;
+    int t1;
+    if (i < NOUT && out_index(i, o, t1)) {
+      const T v = T1[t1];
+      ybase[o] = v;
+      acc = fma((double)xv[k], (double)v, acc);
+    }
+  }
+  const double t = cta_sum<NT>(acc);  // the same branch in every thread of the CTA
+  if (threadIdx.x == 0) *dot = t;
 }
 
 template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
@@ -380,7 +435,8 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   const int tile = blockIdx.x;
   cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz,
                                        tile % Q.ntx, (tile / Q.ntx) % Q.nty,
-                                       tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy);
+                                       tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy,
+                                       Q.dot ? Q.dot + tile : nullptr);
 }
 
 template <int P, typename T>
@@ -489,7 +545,8 @@ void run_batch(const CartesianPlan& proto, const void* d_probs, int nprob, long 
 
 // One launch of the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
 template <int P, typename T, int EX, int EY, int EZ, int NT, int MINB>
-void run_tile(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st) {
+void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse& fuse,
+              cudaStream_t st) {
   using G = Tile<P, EX, EY, EZ, T>;
   CartParams<P, T> Q{};
   fill_eo<P, T>(plan.M, 1.0, Q.Me, Q.Mo);
@@ -507,6 +564,7 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st
   Q.ntx = (plan.nx + EX - 1) / EX;
   Q.nty = (plan.ny + EY - 1) / EY;
   Q.ntz = (plan.nz + EZ - 1) / EZ;
+  Q.dot = fuse.dot;
   const long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
   SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
   const size_t smem = (size_t)G::WORDS * sizeof(T);
@@ -522,7 +580,7 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, cudaStream_t st
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-using RunFn = void (*)(const CartesianPlan&, const void*, void*, cudaStream_t);
+using RunFn = void (*)(const CartesianPlan&, const void*, void*, const CartFuse&, cudaStream_t);
 using BatchFn = void (*)(const CartesianPlan&, const void*, int, long long, unsigned long long*,
                          bool, cudaStream_t);
 struct Candidate {
@@ -675,12 +733,19 @@ void cartesian_apply_candidate(const CartesianPlan& plan, int dtype, int k, cons
                                cudaStream_t stream) {
   SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
   dtype_slot(dtype);
-  pick(plan, dtype, k).run(plan, x, y, stream);
+  pick(plan, dtype, k).run(plan, x, y, CartFuse{}, stream);
 }
 
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
-                     cudaStream_t stream) {
-  cartesian_apply_candidate(plan, dtype, plan.choice[dtype_slot(dtype)], x, y, stream);
+                     cudaStream_t stream, const CartFuse& fuse) {
+  SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
+  pick(plan, dtype, plan.choice[dtype_slot(dtype)]).run(plan, x, y, fuse, stream);
+}
+
+long long cartesian_tiles(const CartesianPlan& plan, int dtype) {
+  const Candidate& c = pick(plan, dtype, plan.choice[dtype_slot(dtype)]);
+  return (long long)((plan.nx + c.ex - 1) / c.ex) * ((plan.ny + c.ey - 1) / c.ey) *
+         ((plan.nz + c.ez - 1) / c.ez);
 }
 
 void cartesian_release(CartesianPlan& plan) { plan.ready = false; }

@@ -3,15 +3,24 @@
 // These replace the host BLAS-1 work of IterativeSolvers.cg! (called at
 // profiling/drivers.jl:85-95). The CG scalars (alpha, beta, dot products)
 // live in a small device array, so an iteration launches without a host
-// round trip. Reductions are deterministic: a fixed grid writes per-block
-// partial sums (FP64 for both vector types), and a one-block kernel adds
-// them in a fixed order.
+// round trip. Reductions are deterministic: every block stores its partial
+// sums (FP64 for both vector types), and the block that finishes last adds
+// all of them in block order, so the result does not depend on which block
+// that is. Elementwise loops take kUnroll elements per thread per round and
+// issue all their loads first, which keeps enough bytes in flight for FP32
+// vectors too.
 #include "sf_cg.cuh"
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace sf {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kUnroll = 4;
 
 // Block-wide sum of NV doubles; returns the totals in thread 0.
 template <int NV>
@@ -35,33 +44,90 @@ __device__ __forceinline__ void block_sum(double (&v)[NV]) {
   }
 }
 
-// partials[b*NV + k]: per-block sums. One block adds them and stores to out[k].
+// Fixed-order sum of partials[b*NV + k] over b < nparts; totals in thread 0.
 template <int NV>
-__global__ void k_finish(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
-  double v[NV];
+__device__ __forceinline__ void sum_partials(const double* partials, long long nparts,
+                                             double (&v)[NV]) {
 #pragma unroll
   for (int k = 0; k < NV; ++k) v[k] = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += kThreads) {
+#pragma unroll 4
+  for (long long b = threadIdx.x; b < nparts; b += kThreads) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] += partials[b * NV + k];
+    for (int k = 0; k < NV; ++k) v[k] += __ldcg(partials + b * NV + k);
   }
   block_sum<NV>(v);
+}
+
+// Each block stores its sums v; the last block to finish adds every block's
+// sums and returns true (in all its threads) with the totals in v (thread 0).
+// The counter is back at zero when the kernel ends.
+template <int NV>
+__device__ __forceinline__ bool last_block_sum(double (&v)[NV], double* partials,
+                                               unsigned int* count) {
+  __shared__ bool is_last;
+  block_sum<NV>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[blockIdx.x * NV + k] = v[k];
+    __threadfence();
+    is_last = atomicAdd(count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  sum_partials<NV>(partials, gridDim.x, v);
+  if (threadIdx.x == 0) *count = 0u;
+  return true;
+}
+
+__device__ __forceinline__ unsigned int* cg_counter(double* s) {
+  return reinterpret_cast<unsigned int*>(s + CG_COUNTER);
+}
+
+// Publishes RR, DONE, ITERS and then the report number to mapped host memory.
+__device__ __forceinline__ void publish(const double* s, double* report) {
+  if (!report) return;
+  report[0] = s[CG_RR];
+  report[1] = s[CG_DONE];
+  report[2] = s[CG_ITERS];
+  __threadfence_system();
+  report[3] = s[CG_REPORTS];
+}
+
+// out = sum of partials in a fixed order (nothing while *skip != 0)
+template <int NV>
+__global__ void k_finish(const double* __restrict__ partials, long long nparts,
+                         double* __restrict__ out, const double* __restrict__ skip) {
+  if (skip && *skip != 0.0) return;
+  double v[NV];
+  sum_partials<NV>(partials, nparts, v);
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) out[k] = v[k];
   }
 }
 
-// out = a . b
+// *out = a . b
 template <typename T>
 __global__ void k_dot(const T* __restrict__ a, const T* __restrict__ b, long long n,
-                      double* __restrict__ partials) {
+                      double* __restrict__ partials, double* __restrict__ out, double* s_count,
+                      const double* __restrict__ skip) {
+  if (skip && *skip != 0.0) return;
+  const long long S = (long long)gridDim.x * kThreads;
+  long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
   double v[1] = {0.0};
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads)
-    v[0] += (double)a[i] * (double)b[i];
-  block_sum<1>(v);
-  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+  for (; i + (kUnroll - 1) * S < n; i += kUnroll * S) {
+    T av[kUnroll], bv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      av[u] = a[i + u * S];
+      bv[u] = b[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) v[0] += (double)av[u] * (double)bv[u];
+  }
+  for (; i < n; i += S) v[0] += (double)a[i] * (double)b[i];
+  if (last_block_sum<1>(v, partials, cg_counter(s_count)) && threadIdx.x == 0) *out = v[0];
 }
 
 // Start of CG: r = b - q (q = A x0, or q = null for x0 = 0), z = dinv r, p = z.
@@ -90,39 +156,119 @@ __global__ void k_cg_start(const T* __restrict__ b, const T* __restrict__ q,
   }
 }
 
-// alpha = s[RZ] / s[PQ]; x += alpha p; r -= alpha q. Sums: (r, dinv r), (r, r).
+__global__ void k_cg_init(double* __restrict__ s, double reltol2) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  s[CG_RZ] = s[CG_RZ_NEW];
+  s[CG_ITERS] = 0.0;
+  s[CG_REPORTS] = 0.0;
+  *cg_counter(s) = 0u;
+  const double bb = s[CG_BB];
+  s[CG_TOL2] = reltol2 < 0.0 ? -1.0 : reltol2 * (bb > 0.0 ? bb : 1.0);
+  const double rr = s[CG_RR];
+  s[CG_DONE] = isfinite(rr) ? (rr <= s[CG_TOL2] ? 2.0 : 0.0) : 3.0;
+}
+
+// alpha = RZ / PQ; r -= alpha q. Sums (r, dinv r) -> RZ_NEW, (r, r) -> RR; then
+// DONE = 1 at convergence, 3 if a sum is not finite.
 template <typename T>
-__global__ void k_cg_update(const double* __restrict__ s, T* __restrict__ x,
-                            const T* __restrict__ p, T* __restrict__ r, const T* __restrict__ q,
-                            const T* __restrict__ dinv, long long n, double* __restrict__ partials) {
-  const double alpha_d = s[CG_RZ] / s[CG_PQ];
-  const T alpha = (T)alpha_d;
+__global__ void k_cg_update(double* __restrict__ s, T* __restrict__ r, const T* __restrict__ q,
+                            const T* __restrict__ dinv, long long n,
+                            double* __restrict__ partials) {
+  if (s[CG_DONE] != 0.0) return;
+  const T alpha = (T)(s[CG_RZ] / s[CG_PQ]);
+  const long long S = (long long)gridDim.x * kThreads;
+  long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    x[i] = fma(alpha, p[i], x[i]);
+  for (; i + (kUnroll - 1) * S < n; i += kUnroll * S) {
+    T qv[kUnroll], rv[kUnroll], dv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      qv[u] = q[i + u * S];
+      rv[u] = r[i + u * S];
+      dv[u] = dinv ? dinv[i + u * S] : T(1);
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const T ri = fma(-alpha, qv[u], rv[u]);
+      r[i + u * S] = ri;
+      const T zi = dinv ? (T)(dv[u] * ri) : ri;
+      v[0] += (double)ri * (double)zi;
+      v[1] += (double)ri * (double)ri;
+    }
+  }
+  for (; i < n; i += S) {
     const T ri = fma(-alpha, q[i], r[i]);
     r[i] = ri;
     const T zi = dinv ? (T)(dinv[i] * ri) : ri;
     v[0] += (double)ri * (double)zi;
     v[1] += (double)ri * (double)ri;
   }
-  block_sum<2>(v);
-  if (threadIdx.x == 0) {
-    partials[blockIdx.x * 2 + 0] = v[0];
-    partials[blockIdx.x * 2 + 1] = v[1];
+  if (last_block_sum<2>(v, partials, cg_counter(s)) && threadIdx.x == 0) {
+    s[CG_RZ_NEW] = v[0];
+    s[CG_RR] = v[1];
+    if (!isfinite(v[1]) || !isfinite(v[0])) s[CG_DONE] = 3.0;
+    else if (v[1] <= s[CG_TOL2]) s[CG_DONE] = 1.0;
   }
 }
 
-// beta = s[RZ_NEW] / s[RZ]; p = dinv r + beta p; then RZ <- RZ_NEW (one thread, after use).
+// x += alpha p; then p = dinv r + beta p unless this iteration converged. The
+// last block ends the iteration: RZ = RZ_NEW, ITERS += 1, DONE 1 -> 2, and a
+// report. A finished solve only reports.
 template <typename T>
-__global__ void k_cg_direction(const double* __restrict__ s, T* __restrict__ p,
-                               const T* __restrict__ r, const T* __restrict__ dinv, long long n) {
+__global__ void k_cg_direction(double* __restrict__ s, T* __restrict__ x, T* __restrict__ p,
+                               const T* __restrict__ r, const T* __restrict__ dinv, long long n,
+                               double* __restrict__ report) {
+  const double done = s[CG_DONE];
+  if (done >= 2.0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      s[CG_REPORTS] += 1.0;
+      publish(s, report);
+    }
+    return;
+  }
+  const T alpha = (T)(s[CG_RZ] / s[CG_PQ]);
   const T beta = (T)(s[CG_RZ_NEW] / s[CG_RZ]);
-  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kThreads) {
-    const T zi = dinv ? (T)(dinv[i] * r[i]) : r[i];
-    p[i] = fma(beta, p[i], zi);
+  const long long S = (long long)gridDim.x * kThreads;
+  long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+  if (done == 0.0) {
+    for (; i + (kUnroll - 1) * S < n; i += kUnroll * S) {
+      T pv[kUnroll], xv[kUnroll], rv[kUnroll], dv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        pv[u] = p[i + u * S];
+        xv[u] = x[i + u * S];
+        rv[u] = r[i + u * S];
+        dv[u] = dinv ? dinv[i + u * S] : T(1);
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        x[i + u * S] = fma(alpha, pv[u], xv[u]);
+        const T zi = dinv ? (T)(dv[u] * rv[u]) : rv[u];
+        p[i + u * S] = fma(beta, pv[u], zi);
+      }
+    }
+    for (; i < n; i += S) {
+      const T pi = p[i];
+      x[i] = fma(alpha, pi, x[i]);
+      const T zi = dinv ? (T)(dinv[i] * r[i]) : r[i];
+      p[i] = fma(beta, pi, zi);
+    }
+  } else {
+    for (; i < n; i += S) x[i] = fma(alpha, p[i], x[i]);
+  }
+  __shared__ bool is_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    is_last = atomicAdd(cg_counter(s), 1u) == gridDim.x - 1;
+    if (is_last) {
+      *cg_counter(s) = 0u;
+      s[CG_RZ] = s[CG_RZ_NEW];
+      s[CG_ITERS] += 1.0;
+      if (done == 1.0) s[CG_DONE] = 2.0;
+      s[CG_REPORTS] += 1.0;
+      publish(s, report);
+    }
   }
 }
 
@@ -172,68 +318,95 @@ __global__ void k_fold(double* __restrict__ x, const float* __restrict__ xs32, l
     x[i] += (double)xs32[i];
 }
 
-int grid_for(long long n) {
+// Blocks of `kernel` resident on the current device at once (cached per device and kernel).
+int resident_blocks(const void* kernel) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> cache;
+  int dev = 0;
+  SF_CUDA_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({dev, kernel});
+  if (it != cache.end()) return it->second;
+  int sms = 0, per_sm = 0;
+  SF_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SF_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+  const int blocks = std::max(1, sms * std::max(1, per_sm));
+  cache[{dev, kernel}] = blocks;
+  return blocks;
+}
+
+// One wave of `kernel` (at most kRedBlocks blocks, the capacity of the partial sums).
+template <typename K>
+int grid_for(K kernel, long long n) {
   long long b = (n + kThreads - 1) / kThreads;
-  if (b > kRedBlocks) b = kRedBlocks;
-  if (b < 1) b = 1;
-  return (int)b;
+  b = std::min<long long>(b, std::min(kRedBlocks, resident_blocks((const void*)kernel)));
+  return (int)std::max(1LL, b);
 }
 
 }  // namespace
 
+void dot_finish(const double* partials, long long nparts, double* out, const double* skip,
+                cudaStream_t st) {
+  k_finish<1><<<1, kThreads, 0, st>>>(partials, nparts, out, skip);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+void cg_reset(double* s, cudaStream_t st) {
+  SF_CUDA_CHECK(cudaMemsetAsync(s, 0, CG_NSLOTS * sizeof(double), st));
+}
+
 template <typename T>
-void vec_dot(const T* a, const T* b, long long n, double* partials, double* out,
-             cudaStream_t st) {
-  const int g = grid_for(n);
-  k_dot<T><<<g, kThreads, 0, st>>>(a, b, n, partials);
-  k_finish<1><<<1, kThreads, 0, st>>>(partials, g, out);
+void vec_dot(const T* a, const T* b, long long n, double* partials, double* out, double* s,
+             const double* skip, cudaStream_t st) {
+  k_dot<T><<<grid_for(k_dot<T>, n), kThreads, 0, st>>>(a, b, n, partials, out, s, skip);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
 template <typename T>
 void cg_start(const T* b, const T* q, const T* dinv, T* r, T* p, long long n, double* partials,
               double* s, cudaStream_t st) {
-  const int g = grid_for(n);
+  const int g = grid_for(k_cg_start<T>, n);
   k_cg_start<T><<<g, kThreads, 0, st>>>(b, q, dinv, r, p, n, partials);
-  k_finish<3><<<1, kThreads, 0, st>>>(partials, g, s + CG_RZ_NEW);  // RZ_NEW, RR, BB
-  k_copy_scalar<<<1, 32, 0, st>>>(s, CG_RZ, CG_RZ_NEW);
+  k_finish<3><<<1, kThreads, 0, st>>>(partials, g, s + CG_RZ_NEW, nullptr);  // RZ_NEW, RR, BB
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+void cg_init(double* s, double reltol2, cudaStream_t st) {
+  k_cg_init<<<1, 32, 0, st>>>(s, reltol2);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
 template <typename T>
-void cg_update(const double* s_in, T* x, const T* p, T* r, const T* q, const T* dinv, long long n,
-               double* partials, double* s, cudaStream_t st) {
-  const int g = grid_for(n);
-  k_cg_update<T><<<g, kThreads, 0, st>>>(s_in, x, p, r, q, dinv, n, partials);
-  k_finish<2><<<1, kThreads, 0, st>>>(partials, g, s + CG_RZ_NEW);  // RZ_NEW, RR
+void cg_update(double* s, T* r, const T* q, const T* dinv, long long n, double* partials,
+               cudaStream_t st) {
+  k_cg_update<T><<<grid_for(k_cg_update<T>, n), kThreads, 0, st>>>(s, r, q, dinv, n, partials);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
 template <typename T>
-void cg_direction(double* s, T* p, const T* r, const T* dinv, long long n, cudaStream_t st) {
-  const int g = grid_for(n);
-  k_cg_direction<T><<<g, kThreads, 0, st>>>(s, p, r, dinv, n);
-  k_copy_scalar<<<1, 32, 0, st>>>(s, CG_RZ, CG_RZ_NEW);
+void cg_direction(double* s, T* x, T* p, const T* r, const T* dinv, long long n, double* report,
+                  cudaStream_t st) {
+  k_cg_direction<T><<<grid_for(k_cg_direction<T>, n), kThreads, 0, st>>>(s, x, p, r, dinv, n, report);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
 template <typename T>
 void vec_invert(const double* d, T* dinv, long long n, cudaStream_t st) {
-  k_invert<T><<<grid_for(n), kThreads, 0, st>>>(d, dinv, n);
+  k_invert<T><<<grid_for(k_invert<T>, n), kThreads, 0, st>>>(d, dinv, n);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
 void mixed_residual(const double* b, const double* q, const float* dinv, float* r32, float* xs32,
                     float* p32, bool set_p, long long n, double* partials, double* s,
                     cudaStream_t st) {
-  const int g = grid_for(n);
+  const int g = grid_for(k_mixed_residual, n);
   k_mixed_residual<<<g, kThreads, 0, st>>>(b, q, dinv, r32, xs32, p32, set_p ? 1 : 0, n, partials);
-  k_finish<2><<<1, kThreads, 0, st>>>(partials, g, s + CG_RZ_NEW);  // RZ_NEW, RR (FP64 true)
+  k_finish<2><<<1, kThreads, 0, st>>>(partials, g, s + CG_RZ_NEW, nullptr);  // RZ_NEW, RR (FP64)
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
 void mixed_fold(double* x, const float* xs32, long long n, cudaStream_t st) {
-  k_fold<<<grid_for(n), kThreads, 0, st>>>(x, xs32, n);
+  k_fold<<<grid_for(k_fold, n), kThreads, 0, st>>>(x, xs32, n);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -242,21 +415,17 @@ void copy_scalar(double* s, int dst, int src, cudaStream_t st) {
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-template void vec_dot<double>(const double*, const double*, long long, double*, double*, cudaStream_t);
-template void vec_dot<float>(const float*, const float*, long long, double*, double*, cudaStream_t);
-template void cg_start<double>(const double*, const double*, const double*, double*, double*,
-                               long long, double*, double*, cudaStream_t);
-template void cg_start<float>(const float*, const float*, const float*, float*, float*, long long,
-                              double*, double*, cudaStream_t);
-template void cg_update<double>(const double*, double*, const double*, double*, const double*,
-                                const double*, long long, double*, double*, cudaStream_t);
-template void cg_update<float>(const double*, float*, const float*, float*, const float*,
-                               const float*, long long, double*, double*, cudaStream_t);
-template void cg_direction<double>(double*, double*, const double*, const double*, long long,
-                                   cudaStream_t);
-template void cg_direction<float>(double*, float*, const float*, const float*, long long,
-                                  cudaStream_t);
-template void vec_invert<double>(const double*, double*, long long, cudaStream_t);
-template void vec_invert<float>(const double*, float*, long long, cudaStream_t);
+#define SF_INST(T)                                                                            \
+  template void vec_dot<T>(const T*, const T*, long long, double*, double*, double*,            \
+                           const double*, cudaStream_t);                                        \
+  template void cg_start<T>(const T*, const T*, const T*, T*, T*, long long, double*, double*,  \
+                            cudaStream_t);                                                      \
+  template void cg_update<T>(double*, T*, const T*, const T*, long long, double*, cudaStream_t); \
+  template void cg_direction<T>(double*, T*, T*, const T*, const T*, long long, double*,        \
+                                cudaStream_t);                                                  \
+  template void vec_invert<T>(const double*, T*, long long, cudaStream_t);
+SF_INST(double)
+SF_INST(float)
+#undef SF_INST
 
 }  // namespace sf

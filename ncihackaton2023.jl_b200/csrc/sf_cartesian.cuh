@@ -15,6 +15,11 @@ struct CartesianPlan {
   int choice[2] = {0, 0};           // tile candidate per dtype (0: FP64, 1: FP32)
 };
 
+// Optional work fused into one apply of the CG loop.
+struct CartFuse {
+  double* dot = nullptr;  // per-tile partial sums of x*y (cartesian_tiles entries)
+};
+
 // Builds the 1D operators; returns false when no tiled kernel exists for SB.
 bool cartesian_prepare(CartesianPlan& plan, int SB, int SQ, const double* A, const double* B,
                        const double* w1, const double* G0, int nx, int ny, int nz);
@@ -39,7 +44,9 @@ void cartesian_batch_launch(const CartesianPlan& proto, int dtype, int cand, con
                             int nprob, long long total, unsigned long long* d_counter, bool iso,
                             cudaStream_t st);
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
-                     cudaStream_t stream);
+                     cudaStream_t stream, const CartFuse& fuse = CartFuse{});
+// Tiles (CTAs) of one apply with the chosen candidate: the entries CartFuse::dot receives.
+long long cartesian_tiles(const CartesianPlan& plan, int dtype);
 void cartesian_release(CartesianPlan& plan);
 
 }  // namespace sf

@@ -7,11 +7,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "sf_cg.cuh"
@@ -43,6 +45,8 @@ struct sf_op {
   double* d_hx = nullptr;    // sf_mul_host staging
   double* d_hy = nullptr;
   double* h_scalar = nullptr;  // pinned
+  double* h_report = nullptr;  // mapped pinned: CG progress reports written by the device
+  double* d_report = nullptr;  // its device address
   double mixed_inner_reltol = 1e-1;
   int last_outer = 0, last_inner = 0;
   double last_relres = 0.0;
@@ -191,13 +195,94 @@ double read_scalar(sf_op* op, const double* d_s, int slot, cudaStream_t st) {
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// The host reads the CG progress reports kCgLag iterations behind the last
+// queued iteration, so the device always has work queued and no iteration
+// waits on the host. The device writes each report into mapped host memory
+// (no copy or event in the stream).
+constexpr int kCgLag = 2;
+constexpr int kStateWords = sf::CG_TOL2 - sf::CG_RR + 1;  // RR, BB, DONE, ITERS, TOL2
+
+// Clears the report buffer (allocated on first use); call with nothing of an
+// earlier solve in flight.
+void reset_reports(sf_op* op) {
+  if (!op->h_report) {
+    SF_CUDA_CHECK(cudaHostAlloc(&op->h_report, 8 * sizeof(double), cudaHostAllocMapped));
+    void* d = nullptr;
+    SF_CUDA_CHECK(cudaHostGetDevicePointer(&d, op->h_report, 0));
+    op->d_report = static_cast<double*>(d);
+  }
+  for (int k = 0; k < 8; ++k) op->h_report[k] = 0.0;
+}
+
+struct Report {
+  double rr, done, iters;
+};
+
+// Waits for report number k (or a later one) and returns it.
+Report wait_report(sf_op* op, int k, cudaStream_t st) {
+  volatile const double* r = op->h_report;
+  for (unsigned spin = 1; r[3] < k; ++spin) {
+    if ((spin & 255) == 0) {
+      const cudaError_t e = cudaStreamQuery(st);
+      if (e == cudaSuccess && r[3] < k)
+        throw Error(SF_ERR_STATE, "CG progress report missing");
+      if (e != cudaSuccess && e != cudaErrorNotReady) SF_CUDA_CHECK(e);
+      std::this_thread::yield();
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return Report{r[0], r[1], r[2]};
+}
+
+// Scalars RR.. now (synchronises the stream).
+const double* read_state(sf_op* op, const double* s, cudaStream_t st) {
+  if (!op->h_scalar) SF_CUDA_CHECK(cudaMallocHost(&op->h_scalar, 8 * sizeof(double)));
+  SF_CUDA_CHECK(cudaMemcpyAsync(op->h_scalar, s + sf::CG_RR, kStateWords * sizeof(double),
+                                cudaMemcpyDeviceToHost, st));
+  SF_CUDA_CHECK(cudaStreamSynchronize(st));
+  return op->h_scalar;
+}
+
+constexpr int kRR = 0, kBB = sf::CG_BB - sf::CG_RR, kDone = sf::CG_DONE - sf::CG_RR,
+              kIters = sf::CG_ITERS - sf::CG_RR;
+
+bool tiled(const sf_op* op, int dtype) {
+  return op->cartesian_ok && sf::cartesian_supported(op->cart, dtype);
+}
+
+// Partial-sum entries the CG reductions of this operator need.
+long long cg_partials(const sf_op* op) {
+  long long n = 3LL * sf::kRedBlocks;
+  for (int dt : {SF_F64, SF_F32})
+    if (tiled(op, dt)) n = std::max(n, sf::cartesian_tiles(op->cart, dt));
+  return n;
+}
+
+// q = A p and s[PQ] = (p, q). The apply itself always runs (after convergence
+// its result is not used); the sum is skipped once s[DONE] != 0. The tiled
+// kernel forms per-tile partial sums in its store phase.
+template <typename T>
+void apply_pq(sf_op* op, const T* p, T* q, double* partials, double* s, cudaStream_t st) {
+  const int dtype = sizeof(T) == 8 ? SF_F64 : SF_F32;
+  if (tiled(op, dtype)) {
+    sf::CartFuse fuse;
+    fuse.dot = partials;
+    sf::cartesian_apply(op->cart, dtype, p, q, st, fuse);
+    sf::dot_finish(partials, sf::cartesian_tiles(op->cart, dtype), s + sf::CG_PQ,
+                   s + sf::CG_DONE, st);
+  } else {
+    apply_impl(op, dtype, p, q, st);
+    sf::vec_dot<T>(p, q, op->n_free, partials, s + sf::CG_PQ, s, s + sf::CG_DONE, st);
+  }
+}
+
 // Plain or Jacobi FP64 CG. Returns iterations; sets relres.
 int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, int maxiter,
            double* relres, cudaStream_t st) {
   const long long n = op->n_free;
   const size_t vb = align256(n * sizeof(double));
   const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
-  const size_t pb = align256(sf::kRedBlocks * 3 * sizeof(double));
+  const size_t pb = align256(cg_partials(op) * sizeof(double));
   char* ws = static_cast<char*>(workspace(op, 4 * vb + sb + pb));
   double* r = reinterpret_cast<double*>(ws);
   double* p = reinterpret_cast<double*>(ws + vb);
@@ -210,25 +295,26 @@ int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, in
     sf::vec_invert<double>(op->d_diag, dinv, n, st);
   }
   const double* Dv = jacobi ? dinv : nullptr;
+  sf::cg_reset(s, st);
   apply_impl(op, SF_F64, x, q, st);
   sf::cg_start<double>(b, q, Dv, r, p, n, partials, s, st);
-  double bb = read_scalar(op, s, sf::CG_BB, st);
-  double rr = read_scalar(op, s, sf::CG_RR, st);
+  sf::cg_init(s, reltol * reltol, st);
+  const double* h = read_state(op, s, st);
+  const double bb = h[kBB];
   const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
-  const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
-  int it = 0;
-  while (rr > tol2 && it < maxiter) {
-    apply_impl(op, SF_F64, p, q, st);
-    sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, st);
-    sf::cg_update<double>(s, x, p, r, q, Dv, n, partials, s, st);
-    rr = read_scalar(op, s, sf::CG_RR, st);
+  double done = h[kDone];
+  reset_reports(op);
+  for (int it = 0; it < maxiter && done == 0.0;) {
+    apply_pq<double>(op, p, q, partials, s, st);
+    sf::cg_update<double>(s, r, q, Dv, n, partials, st);
+    sf::cg_direction<double>(s, x, p, r, Dv, n, op->d_report, st);
     ++it;
-    SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in CG");
-    if (rr <= tol2) break;
-    sf::cg_direction<double>(s, p, r, Dv, n, st);
+    if (it > kCgLag) done = wait_report(op, it - kCgLag, st).done;
   }
-  *relres = std::sqrt(rr) / nb;
-  return it;
+  h = read_state(op, s, st);
+  SF_REQUIRE(h[kDone] != 3.0, SF_ERR_NONFINITE, "non-finite residual in CG");
+  *relres = std::sqrt(h[kRR]) / nb;
+  return (int)h[kIters];
 }
 
 // Mixed-precision Jacobi CG with reliable updates. The CG recurrence (p, q,
@@ -237,14 +323,16 @@ int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, in
 // `mixed_inner_reltol` since the last update (or below the target), the
 // partial solution is folded into the FP64 solution x, and the FP64 true
 // residual b - A64 x replaces r. The search direction is kept, so the Krylov
-// recurrence is not restarted. The stopping test uses the FP64 true residual only.
+// recurrence is not restarted. The stopping test uses the FP64 true residual
+// only. The host reads the FP32 residual kCgLag iterations late, so an update
+// comes up to kCgLag iterations after the drop that triggers it.
 int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, double* relres,
              int* outer_out, cudaStream_t st) {
   const long long n = op->n_free;
   const size_t v8 = align256(n * sizeof(double));
   const size_t v4 = align256(n * sizeof(float));
   const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
-  const size_t pb = align256(sf::kRedBlocks * 3 * sizeof(double));
+  const size_t pb = align256(cg_partials(op) * sizeof(double));
   char* ws = static_cast<char*>(workspace(op, v8 + 5 * v4 + sb + pb));
   double* q64 = reinterpret_cast<double*>(ws);
   char* w4 = ws + v8;
@@ -257,41 +345,48 @@ int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, 
   double* partials = reinterpret_cast<double*>(ws + v8 + 5 * v4 + sb);
   ensure_diag(op, st);
   sf::vec_invert<float>(op->d_diag, dinv32, n, st);
-  sf::vec_dot<double>(b, b, n, partials, s + sf::CG_BB, st);
-  const double bb = read_scalar(op, s, sf::CG_BB, st);
+  sf::cg_reset(s, st);
+  sf::vec_dot<double>(b, b, n, partials, s + sf::CG_BB, s, nullptr, st);
+  // true residual of the initial guess; p = dinv r; the device never stops on its own
+  apply_impl(op, SF_F64, x, q64, st);
+  sf::mixed_residual(b, q64, dinv32, r32, xs32, p32, true, n, partials, s, st);
+  sf::cg_init(s, -1.0, st);
+  const double* h = read_state(op, s, st);
+  const double bb = h[kBB];
   const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
   const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
   const double delta2 = op->mixed_inner_reltol * op->mixed_inner_reltol;
-  // true residual of the initial guess; p = dinv r
-  apply_impl(op, SF_F64, x, q64, st);
-  sf::mixed_residual(b, q64, dinv32, r32, xs32, p32, true, n, partials, s, st);
-  sf::copy_scalar(s, sf::CG_RZ, sf::CG_RZ_NEW, st);
-  double rr64 = read_scalar(op, s, sf::CG_RR, st);
+  double rr64 = h[kRR];
   SF_REQUIRE(std::isfinite(rr64), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
   double rr_ref = rr64;
-  int it = 0, updates = 0;
+  int it = 0, updates = 0, last_update = 0;
   bool dirty = false;  // xs32 holds a partial solution not yet folded into x
+  reset_reports(op);
   while (rr64 > tol2 && it < maxiter) {
-    apply_impl(op, SF_F32, p32, q32, st);
-    sf::vec_dot<float>(p32, q32, n, partials, s + sf::CG_PQ, st);
-    sf::cg_update<float>(s, xs32, p32, r32, q32, dinv32, n, partials, s, st);
-    const double rr = read_scalar(op, s, sf::CG_RR, st);
+    apply_pq<float>(op, p32, q32, partials, s, st);
+    sf::cg_update<float>(s, r32, q32, dinv32, n, partials, st);
+    sf::cg_direction<float>(s, xs32, p32, r32, dinv32, n, op->d_report, st);
     ++it;
     dirty = true;
-    SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
-    if (rr <= delta2 * rr_ref || rr <= tol2 || it >= maxiter) {
+    bool refine = it >= maxiter;
+    if (it - kCgLag > last_update) {  // residuals from before the last update do not count
+      const Report rep = wait_report(op, it - kCgLag, st);
+      SF_REQUIRE(rep.done != 3.0, SF_ERR_NONFINITE, "non-finite residual in mixed CG");
+      refine = refine || rep.rr <= delta2 * rr_ref || rep.rr <= tol2;
+    }
+    if (refine) {
       // reliable update: fold xs into x, replace r by the FP64 true residual
       sf::mixed_fold(x, xs32, n, st);
       apply_impl(op, SF_F64, x, q64, st);
       sf::mixed_residual(b, q64, dinv32, r32, xs32, p32, false, n, partials, s, st);
-      rr64 = read_scalar(op, s, sf::CG_RR, st);
+      sf::copy_scalar(s, sf::CG_RZ, sf::CG_RZ_NEW, st);
+      rr64 = read_state(op, s, st)[kRR];
       SF_REQUIRE(std::isfinite(rr64), SF_ERR_NONFINITE, "non-finite residual in mixed CG");
       rr_ref = rr64;
+      last_update = it;
       dirty = false;
       ++updates;
-      if (rr64 <= tol2) break;
     }
-    sf::cg_direction<float>(s, p32, r32, dinv32, n, st);
   }
   if (dirty) sf::mixed_fold(x, xs32, n, st);
   *relres = std::sqrt(rr64) / nb;
@@ -371,6 +466,7 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_hx);
   dfree(op->d_hy);
   if (op->h_scalar) cudaFreeHost(op->h_scalar);
+  if (op->h_report) cudaFreeHost(op->h_report);
   sf::cartesian_release(op->cart);
   delete op;
   return SF_OK;
@@ -810,6 +906,7 @@ constexpr long long kNoAllocScalarWords = 32;  // CG scalars, padded to 256 byte
 constexpr long long kNoAllocWords =
     5 * kNoAllocMaxFree + kNoAllocScalarWords + 3LL * sf::kRedBlocks;
 static_assert((kNoAllocMaxFree * 8) % 256 == 0, "scratch vectors must stay 256-byte aligned");
+static_assert(sf::CG_NSLOTS <= kNoAllocScalarWords, "CG scalars exceed their scratch words");
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocWords];
 
@@ -858,25 +955,23 @@ int cg_f64_noalloc(sf_op* op, bool jacobi, const double* b, double* x, double re
     sf::vec_invert<double>(diag, dinv, n, st);
   }
   const double* Dv = jacobi ? dinv : nullptr;
+  sf::cg_reset(s, st);
   apply_impl(op, SF_F64, x, q, st);
   sf::cg_start<double>(b, q, Dv, r, p, n, partials, s, st);
+  sf::cg_init(s, reltol * reltol, st);
   const double bb = read_scalar_noalloc(s, sf::CG_BB, st);
-  double rr = read_scalar_noalloc(s, sf::CG_RR, st);
   const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
-  const double tol2 = reltol * reltol * (bb > 0 ? bb : 1.0);
-  int it = 0;
-  while (rr > tol2 && it < maxiter) {
+  double done = read_scalar_noalloc(s, sf::CG_DONE, st);
+  for (int it = 0; it < maxiter && done == 0.0; ++it) {
     apply_impl(op, SF_F64, p, q, st);
-    sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, st);
-    sf::cg_update<double>(s, x, p, r, q, Dv, n, partials, s, st);
-    rr = read_scalar_noalloc(s, sf::CG_RR, st);
-    ++it;
-    SF_REQUIRE(std::isfinite(rr), SF_ERR_NONFINITE, "non-finite residual in CG");
-    if (rr <= tol2) break;
-    sf::cg_direction<double>(s, p, r, Dv, n, st);
+    sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, s, s + sf::CG_DONE, st);
+    sf::cg_update<double>(s, r, q, Dv, n, partials, st);
+    sf::cg_direction<double>(s, x, p, r, Dv, n, nullptr, st);
+    done = read_scalar_noalloc(s, sf::CG_DONE, st);
   }
-  *relres = std::sqrt(rr) / nb;
-  return it;
+  SF_REQUIRE(done != 3.0, SF_ERR_NONFINITE, "non-finite residual in CG");
+  *relres = std::sqrt(read_scalar_noalloc(s, sf::CG_RR, st)) / nb;
+  return (int)read_scalar_noalloc(s, sf::CG_ITERS, st);
 }
 
 }  // namespace

@@ -82,3 +82,36 @@ def test_deformed_q8_iterations_match_oracle(sf):
     # kappa(A) is large, so rounding differences move the count a little
     assert info["converged"] and abs(info["iters"] - it_ref) <= max(10, it_ref // 10)
     assert np.abs(x.cpu().numpy() - x_ref).max() < 1e-6 * np.abs(x_ref).max()
+
+
+@pytest.mark.parametrize("mode", ["jacobi", "mixed"])
+def test_cg_is_deterministic(sf, mode):
+    """The reductions add partial sums in a fixed order, so a repeated solve
+    gives the same iterates bit for bit (tiled Cartesian path, Q4)."""
+    import torch
+    A, V, om, mesh, b, bd = setup(sf, 4, 8, 6)
+    assert A.uses_tiled_kernel()
+    x1, i1 = sf.cg(A, bd, reltol=1e-10, mode=mode)
+    x2, i2 = sf.cg(A, bd, reltol=1e-10, mode=mode)
+    assert i1["iters"] == i2["iters"] and i1["relres"] == i2["relres"]
+    assert torch.equal(x1, x2)
+
+
+def test_cg_tiled_and_general_paths_agree(sf):
+    """The tiled kernel (fused (p, Ap) reduction) and the general kernel
+    (separate reduction) drive the same Jacobi CG."""
+    import torch
+    A, V, om, mesh, b, bd = setup(sf, 3, 6, 5)
+    assert A.uses_tiled_kernel()
+    x_t, i_t = sf.cg(A, bd, reltol=1e-11, mode="jacobi")
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (5, 5, 5), perturb=0.0, seed=1)
+    Vr = sf.FESpace(model, 3, renumber_seed=7)
+    m = sf.SumFactorizationMap(3, (3,) * 3, (6,) * 3)
+    Ag = sf.LazyMatrix(m, Vr, Vr, sf.Measure(model, 6))
+    assert not Ag.uses_tiled_kernel()
+    perm = torch.from_numpy(Vr.perm).cuda()  # lexicographic index -> renumbered id
+    bg = torch.empty_like(bd)
+    bg[perm] = bd
+    x_g, i_g = sf.cg(Ag, bg, reltol=1e-11, mode="jacobi")
+    assert abs(i_t["iters"] - i_g["iters"]) <= 1
+    assert (x_g[perm] - x_t).abs().max().item() < 1e-9 * x_t.abs().max().item()
