@@ -57,6 +57,12 @@ def parse():
     ap.add_argument("--cg-only", action="store_true",
                     help="only the CG solves (autotuned tiles; no apply leg): for profiling")
     ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
+    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8"], default=None,
+                    help="run only this secondary configuration (no apply leg): for profiling")
+    ap.add_argument("--deformed-cells", type=int, default=32,
+                    help="cells per direction of the deformed Q8 section")
+    ap.add_argument("--deformed-cg", type=int, default=1500,
+                    help="CG iteration budget of the deformed Q8 section (0: no CG)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-secondary", action="store_true",
@@ -201,6 +207,11 @@ def run_ours(args, rank, world, local_rank):
     sf = g.load()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if args.section is not None:
+        fn = {"batched": run_batched, "adjoint": run_adjoint,
+              "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,
+                                                            cg_iters=args.deformed_cg)}
+        return {args.section: fn[args.section](sf, dev)}
     m, model, V, A = build_problem(sf)
     if args.cg_only:
         A.autotune(torch.float64)
@@ -478,7 +489,7 @@ def run_adjoint(sf, dev, n=32, p=3, seed=11):
             "fd_rel_err": abs(fd - ad) / abs(fd)}
 
 
-def run_deformed(sf, dev, n=32, p=8, seed=5):
+def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
     """Q8 on 32^3 cells, interior vertices moved by U[-0.2h, 0.2h] (seeded),
     9-point Gauss, per-point symmetric metric (6 FP64 values) stored: FP64 and
     FP32 apply times and bytes moved, and CG to 1e-10 (FP64 and mixed)."""
@@ -510,10 +521,10 @@ def run_deformed(sf, dev, n=32, p=8, seed=5):
     # is ~5e6 on 3^3 cells already and grows like h^-2, so Jacobi CG cannot reach
     # 1e-10 here in a bounded time. Report the residual reached after a fixed
     # iteration budget in FP64 and in mixed precision.
-    res["cg_budget_iters"] = 1500
-    for mode, key in (("jacobi", "f64"), ("mixed", "mixed")):
+    res["cg_budget_iters"] = cg_iters
+    for mode, key in ((("jacobi", "f64"), ("mixed", "mixed")) if cg_iters > 0 else ()):
         t0 = time.perf_counter()
-        _, info = sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=1500, raise_on_fail=False)
+        _, info = sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=cg_iters, raise_on_fail=False)
         torch.cuda.synchronize()
         res[f"cg_{key}"] = {"s": round(time.perf_counter() - t0, 3), "iters": info["iters"],
                             "relres": info["relres"], "converged": info["converged"]}

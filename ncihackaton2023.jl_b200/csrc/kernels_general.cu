@@ -51,6 +51,9 @@ struct Shape {
   static constexpr int SE = S0 + 2 * S1 + 3 * S2;        // words per element
   static constexpr int EPB = (256 / NL) > 0 ? (256 / NL) : 1;  // elements per block
   static constexpr int THREADS = EPB * NL;
+  static constexpr int SM3 = SM * SM * SM;
+  static constexpr int SL = 3 * SM3;  // words per element of k_general (three padded slots)
+  static constexpr int MINB = 2;      // CTAs per SM asked of the register allocator
 };
 
 // Global free index of tensor position `pos` of cell `c` on the structured mesh, or -1.
@@ -71,13 +74,13 @@ __device__ __forceinline__ long long structured_index(long long c, int pos, int 
 template <typename T>
 __device__ __forceinline__ void atomic_add(T* a, T v) { atomicAdd(a, v); }
 
-// FP64 FMAs cannot take a 64-bit operand from the constant bank. At high
-// order (SQ*SB >= 64) the FP64 1D matrices are therefore staged once per CTA
-// in shared memory and read with broadcast loads; keeping 2*SQ*SB doubles in
-// registers would cost up to 162 registers per thread at Q8. At lower orders,
-// and in FP32, they are read straight from the kernel parameters.
+// FP64 FMAs cannot take a 64-bit operand from the constant bank, so the FP64
+// 1D matrices are staged once per CTA in shared memory and read with
+// broadcast loads; keeping 2*SQ*SB doubles in registers would cost up to 162
+// registers per thread at Q8. FP32 reads them straight from the kernel
+// parameters below SQ*SB = 64.
 template <typename T, int SB, int SQ>
-constexpr bool kStageMats = sizeof(T) == 8 && SQ * SB >= 64;
+constexpr bool kStageMats = sizeof(T) == 8 ? SQ * SB >= 16 : SQ * SB >= 64;
 #define MA(i) (kStageMats<T, SB, SQ> ? sMat[(i)] : P.A[(i)])
 #define MB(i) (kStageMats<T, SB, SQ> ? sMat[SQ * SB + (i)] : P.B[(i)])
 
@@ -91,24 +94,65 @@ __device__ __forceinline__ void stage_mats(const GenParams<SB, SQ, T>& P, T* sMa
   }
 }
 
+// Element kernel. Shared memory per element is three slots U0, U1, U2 of
+// SM^3 words each, indexed (c3 * SM + c2) * SM + c1 with c1 fastest. Every
+// pass gives a thread whole 1D lines, and the line's inputs and outputs sit at
+// the same slot positions (the padding to SM makes that true for SB != SQ),
+// so each pass works in place on positions no other thread touches:
+//   gather      U0 = X
+//   forward x   lines (j,k):   U1 = A1 = A X,  U2 = B1 = B X
+//   forward y   lines (qi,k):  U1 = AA = A A1, U0 = AB = B A1, U2 = BA = A B1
+//   z           lines (qi,qj): u = (A BA, A AB, B AA) in place, one component at a
+//               time; v = G(q) u point by point; the transposes back, again one
+//               component at a time (the same thread, so no barrier in between)
+//   backward y  lines (qi,k):  U1 = A1 = A^T AA + B^T AB,  U2 = B1 = A^T BA
+//   backward x  lines (j,k):   U0 = Y = A^T A1 + B^T B1
+// A thread holds at most 2 lines (18 values at Q8) in registers, which keeps
+// several CTAs resident per SM to hide the latency of the per-point metric.
 template <int SB, int SQ, typename T>
-__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS)
+__device__ __forceinline__ void line_apply(const T* sMat, const GenParams<SB, SQ, T>& P, int rows,
+                                           int cols, bool transpose, bool useB, T* io, int stride) {
+  // io[r * stride] (r < rows) = sum_c M[r][c] io[c * stride] (c < cols), M = A or B
+  // stored [q][basis]; transpose: M^T. Inputs are read before any output is written.
+  constexpr int N = SB > SQ ? SB : SQ;
+  T in[N];
+  // keeps the compiler from overlapping consecutive line passes (which would
+  // hold several lines in registers at once)
+  asm volatile("" ::: "memory");
+#pragma unroll
+  for (int c = 0; c < N; ++c)
+    if (c < cols) in[c] = io[c * stride];
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    if (r >= rows) break;
+    T acc = T(0);
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+      if (c >= cols) break;
+      const int ix = transpose ? c * SB + r : r * SB + c;
+      acc = fma(useB ? MB(ix) : MA(ix), in[c], acc);
+    }
+    io[r * stride] = acc;
+  }
+}
+
+template <int SB, int SQ, typename T>
+__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS, Shape<SB, SQ>::MINB)
 k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   using S = Shape<SB, SQ>;
+  constexpr int SM = S::SM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int el = threadIdx.x / S::NL;
   const int l = threadIdx.x % S::NL;
   const long long cell = (long long)blockIdx.x * S::EPB + el;
   const bool valid = cell < P.ncells;
 
-  T* X = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SE;
-  T* A1 = X + S::S0;
-  T* B1 = A1 + S::S1;
-  T* AA = B1 + S::S1;
-  T* AB = AA + S::S2;
-  T* BA = AB + S::S2;
+  T* U0 = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SL;
+  T* U1 = U0 + S::SM3;
+  T* U2 = U1 + S::SM3;
   __shared__ T sMat[kStageMats<T, SB, SQ> ? 2 * SQ * SB : 1];
   stage_mats<SB, SQ, T>(P, sMat);  // visible after the first __syncthreads below
+  auto at = [](int c3, int c2, int c1) { return (c3 * SM + c2) * SM + c1; };
 
   // ---------------- gather ----------------
   for (int pos = l; pos < S::S0; pos += S::NL) {
@@ -125,16 +169,17 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
         if (id >= 0) v = P.x[id];
       }
     }
-    X[pos] = v;
+    const int i = pos % SB, j = (pos / SB) % SB, k = pos / (SB * SB);
+    U0[at(k, j, i)] = v;
   }
   __syncthreads();
 
   // ---------------- forward x: lines (j,k), contract i ----------------
   if (l < SB * SB) {
-    const int line = l;  // = j + SB*k
+    const int j = l % SB, k = l / SB;
     T in[SB];
 #pragma unroll
-    for (int i = 0; i < SB; ++i) in[i] = X[line * SB + i];
+    for (int i = 0; i < SB; ++i) in[i] = U0[at(k, j, i)];
 #pragma unroll
     for (int qi = 0; qi < SQ; ++qi) {
       T a = T(0), b = T(0);
@@ -143,8 +188,8 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
         a = fma(MA(qi * SB + i), in[i], a);
         b = fma(MB(qi * SB + i), in[i], b);
       }
-      A1[line * SQ + qi] = a;
-      B1[line * SQ + qi] = b;
+      U1[at(k, j, qi)] = a;
+      U2[at(k, j, qi)] = b;
     }
   }
   __syncthreads();
@@ -152,124 +197,100 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   // ---------------- forward y: lines (qi,k), contract j ----------------
   if (l < SQ * SB) {
     const int qi = l % SQ, k = l / SQ;
-    T a1[SB], b1[SB];
+    {
+      T a1[SB];
 #pragma unroll
-    for (int j = 0; j < SB; ++j) {
-      a1[j] = A1[(k * SB + j) * SQ + qi];
-      b1[j] = B1[(k * SB + j) * SQ + qi];
-    }
+      for (int j = 0; j < SB; ++j) a1[j] = U1[at(k, j, qi)];
 #pragma unroll
-    for (int qj = 0; qj < SQ; ++qj) {
-      T aa = T(0), ab = T(0), ba = T(0);
+      for (int qj = 0; qj < SQ; ++qj) {
+        T aa = T(0), ab = T(0);
 #pragma unroll
-      for (int j = 0; j < SB; ++j) {
-        aa = fma(MA(qj * SB + j), a1[j], aa);
-        ab = fma(MB(qj * SB + j), a1[j], ab);
-        ba = fma(MA(qj * SB + j), b1[j], ba);
+        for (int j = 0; j < SB; ++j) {
+          aa = fma(MA(qj * SB + j), a1[j], aa);
+          ab = fma(MB(qj * SB + j), a1[j], ab);
+        }
+        U1[at(k, qj, qi)] = aa;
+        U0[at(k, qj, qi)] = ab;
       }
-      const int o = (k * SQ + qj) * SQ + qi;
-      AA[o] = aa;
-      AB[o] = ab;
-      BA[o] = ba;
     }
+    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, false, U2 + at(k, 0, qi), SM);  // BA = A B1
   }
   __syncthreads();
 
-  // ------- forward z, metric, backward z: lines (qi,qj), registers -------
+  // ------------- z: forward, metric, backward; lines (qi,qj) -------------
   if (l < SQ * SQ) {
     const int qi = l % SQ, qj = l / SQ;
-    T ba[SB], ab[SB], aa[SB];
-#pragma unroll
-    for (int k = 0; k < SB; ++k) {
-      const int o = (k * SQ + qj) * SQ + qi;
-      ba[k] = BA[o];
-      ab[k] = AB[o];
-      aa[k] = AA[o];
-    }
-    T ba_o[SB], ab_o[SB], aa_o[SB];
-#pragma unroll
-    for (int k = 0; k < SB; ++k) ba_o[k] = ab_o[k] = aa_o[k] = T(0);
-#pragma unroll
+    T* zx = U2 + at(0, qj, qi);  // BA -> ux -> vx -> back
+    T* zy = U0 + at(0, qj, qi);  // AB -> uy -> vy -> back
+    T* zz = U1 + at(0, qj, qi);  // AA -> uz -> vz -> back
+    constexpr int ZS = SM * SM;
+    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, false, zx, ZS);
+    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, false, zy, ZS);
+    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, true, zz, ZS);
+    // metric in FP64 (geometric factors are kept in FP64 for both dtypes)
+    const double* gt = P.geom == GEOM_SEPARABLE ? nullptr : P.gtab + (valid ? cell : 0) * P.gstride;
+#pragma unroll 3
     for (int qk = 0; qk < SQ; ++qk) {
-      T ux = T(0), uy = T(0), uz = T(0);
-#pragma unroll
-      for (int k = 0; k < SB; ++k) {
-        ux = fma(MA(qk * SB + k), ba[k], ux);
-        uy = fma(MA(qk * SB + k), ab[k], uy);
-        uz = fma(MB(qk * SB + k), aa[k], uz);
-      }
-      // metric in FP64 (geometric factors are kept in FP64 for both dtypes)
       const int q = qi + SQ * (qj + SQ * qk);
       double g[6];
+      asm volatile("" ::: "memory");
       if (P.geom == GEOM_SEPARABLE) {
         const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
 #pragma unroll
         for (int c = 0; c < 6; ++c) g[c] = s * P.G0[c];
       } else {
-        const double* gt = P.gtab + (valid ? cell : 0) * P.gstride;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) g[c] = gt[c * SQ * SQ * SQ + q];
+        for (int c = 0; c < 6; ++c) g[c] = __ldg(gt + c * SQ * SQ * SQ + q);
       }
       if (P.kappa) {
         const double kq = valid ? P.kappa[cell * (SQ * SQ * SQ) + q] : 0.0;
 #pragma unroll
         for (int c = 0; c < 6; ++c) g[c] *= kq;
       }
-      const double dx = (double)ux, dy = (double)uy, dz = (double)uz;
-      const T vx = (T)(g[0] * dx + g[3] * dy + g[4] * dz);
-      const T vy = (T)(g[3] * dx + g[1] * dy + g[5] * dz);
-      const T vz = (T)(g[4] * dx + g[5] * dy + g[2] * dz);
-#pragma unroll
-      for (int k = 0; k < SB; ++k) {
-        ba_o[k] = fma(MA(qk * SB + k), vx, ba_o[k]);
-        ab_o[k] = fma(MA(qk * SB + k), vy, ab_o[k]);
-        aa_o[k] = fma(MB(qk * SB + k), vz, aa_o[k]);
-      }
+      const double dx = (double)zx[qk * ZS], dy = (double)zy[qk * ZS], dz = (double)zz[qk * ZS];
+      zx[qk * ZS] = (T)(g[0] * dx + g[3] * dy + g[4] * dz);
+      zy[qk * ZS] = (T)(g[3] * dx + g[1] * dy + g[5] * dz);
+      zz[qk * ZS] = (T)(g[4] * dx + g[5] * dy + g[2] * dz);
     }
-#pragma unroll
-    for (int k = 0; k < SB; ++k) {
-      const int o = (k * SQ + qj) * SQ + qi;
-      BA[o] = ba_o[k];
-      AB[o] = ab_o[k];
-      AA[o] = aa_o[k];
-    }
+    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, false, zx, ZS);
+    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, false, zy, ZS);
+    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, true, zz, ZS);
   }
   __syncthreads();
 
-  // ---------------- backward y: lines (qi,k) ----------------
+  // ---------------- backward y: lines (qi,k), contract qj ----------------
   if (l < SQ * SB) {
     const int qi = l % SQ, k = l / SQ;
-    T aa[SQ], ab[SQ], ba[SQ];
-#pragma unroll
-    for (int qj = 0; qj < SQ; ++qj) {
-      const int o = (k * SQ + qj) * SQ + qi;
-      aa[qj] = AA[o];
-      ab[qj] = AB[o];
-      ba[qj] = BA[o];
-    }
-#pragma unroll
-    for (int j = 0; j < SB; ++j) {
-      T a1 = T(0), b1 = T(0);
+    {
+      T aa[SQ], ab[SQ];
 #pragma unroll
       for (int qj = 0; qj < SQ; ++qj) {
-        a1 = fma(MA(qj * SB + j), aa[qj], a1);
-        a1 = fma(MB(qj * SB + j), ab[qj], a1);
-        b1 = fma(MA(qj * SB + j), ba[qj], b1);
+        aa[qj] = U1[at(k, qj, qi)];
+        ab[qj] = U0[at(k, qj, qi)];
       }
-      A1[(k * SB + j) * SQ + qi] = a1;
-      B1[(k * SB + j) * SQ + qi] = b1;
+#pragma unroll
+      for (int j = 0; j < SB; ++j) {
+        T a1 = T(0);
+#pragma unroll
+        for (int qj = 0; qj < SQ; ++qj) {
+          a1 = fma(MA(qj * SB + j), aa[qj], a1);
+          a1 = fma(MB(qj * SB + j), ab[qj], a1);
+        }
+        U1[at(k, j, qi)] = a1;
+      }
     }
+    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, false, U2 + at(k, 0, qi), SM);  // B1 = A^T BA
   }
   __syncthreads();
 
-  // ---------------- backward x: lines (j,k) -> Y in X ----------------
+  // ---------------- backward x: lines (j,k) -> Y in U0 ----------------
   if (l < SB * SB) {
-    const int line = l;
+    const int j = l % SB, k = l / SB;
     T a1[SQ], b1[SQ];
 #pragma unroll
     for (int qi = 0; qi < SQ; ++qi) {
-      a1[qi] = A1[line * SQ + qi];
-      b1[qi] = B1[line * SQ + qi];
+      a1[qi] = U1[at(k, j, qi)];
+      b1[qi] = U2[at(k, j, qi)];
     }
 #pragma unroll
     for (int i = 0; i < SB; ++i) {
@@ -279,7 +300,7 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
         yv = fma(MA(qi * SB + i), a1[qi], yv);
         yv = fma(MB(qi * SB + i), b1[qi], yv);
       }
-      X[line * SB + i] = yv;
+      U0[at(k, j, i)] = yv;
     }
   }
   __syncthreads();
@@ -287,7 +308,8 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   // ---------------- scatter ----------------
   if (!valid) return;
   for (int pos = l; pos < S::S0; pos += S::NL) {
-    const T v = X[pos];
+    const int i = pos % SB, j = (pos / SB) % SB, k = pos / (SB * SB);
+    const T v = U0[at(k, j, i)];
     if (P.mode == 1) {
       P.y[cell * S::S0 + P.t2l[pos]] = v;
     } else if (P.ids) {
@@ -539,7 +561,7 @@ void run_general(int mode, const double* A, const double* B, const Cells& cells,
     SF_CUDA_CHECK(cudaGetLastError());
     return;
   }
-  const size_t smem = (size_t)S::EPB * S::SE * sizeof(T);
+  const size_t smem = (size_t)S::EPB * S::SL * sizeof(T);
   SF_CUDA_CHECK(cudaFuncSetAttribute(k_general<SB, SQ, T>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long blocks = (ncells + S::EPB - 1) / S::EPB;
