@@ -17,15 +17,36 @@
 // __grid_constant__ parameters (staged in shared memory for FP64 at high order,
 // see kStageMats). The scatter-add uses atomics into a y that was zeroed before
 // the launch. Dirichlet dofs (id < 0) read as zero and are skipped.
+#include <cmath>
+#include <type_traits>
+
 #include "sf_internal.cuh"
 
 namespace sf {
 namespace {
 
+// Even-odd tables of one R x C operator M with M[R-1-r][C-1-c] = sign M[r][c]
+// (A and A^T: sign +1; B and B^T: sign -1). Row r < HR holds the pairs
+// (E[r][i], O[r][i]) for i < HC, with E[r][i] = (M[r][i] + M[r][C-1-i]) / 2 and
+// O[r][i] = (M[r][i] - M[r][C-1-i]) / 2, then (M[r][HC], 0) when C is odd, so
+// that one 2-wide shared load fetches a pair. Row length W is even.
+template <int R, int C>
+struct EOT {
+  static constexpr int HR = (R + 1) / 2, HC = C / 2, MC = C % 2, W = 2 * HC + 2 * MC;
+  static constexpr int N = HR * W;
+};
+template <int SB, int SQ>
+struct EOTables {  // offsets of the tables of A, B (SQ x SB) and A^T, B^T (SB x SQ)
+  static constexpr int NA = EOT<SQ, SB>::N, NT = EOT<SB, SQ>::N;
+  static constexpr int OFF[4] = {0, NA, 2 * NA, 2 * NA + NT};
+  static constexpr int TOTAL = 2 * NA + 2 * NT;
+};
+
 template <int SB, int SQ, typename T>
 struct GenParams {
   T A[SQ * SB];  // [qp][basis]
   T B[SQ * SB];
+  T eo[EOTables<SB, SQ>::TOTAL];  // even-odd tables (used when A and B are symmetric)
   double w1[SQ];
   double G0[6];
   const T* x;
@@ -48,7 +69,6 @@ struct Shape {
   static constexpr int S0 = SB * SB * SB;                // X / Y
   static constexpr int S1 = SB * SB * SQ;                // each of A1, B1
   static constexpr int S2 = SB * SQ * SQ;                // each of AA, AB, BA
-  static constexpr int SE = S0 + 2 * S1 + 3 * S2;        // words per element
   static constexpr int EPB = (256 / NL) > 0 ? (256 / NL) : 1;  // elements per block
   static constexpr int THREADS = EPB * NL;
   static constexpr int SM3 = SM * SM * SM;
@@ -69,6 +89,26 @@ __device__ __forceinline__ long long structured_index(long long c, int pos, int 
   const int Nx = nx * p, Ny = ny * p, Nz = nz * p;
   if (gx <= 0 || gx >= Nx || gy <= 0 || gy >= Ny || gz <= 0 || gz >= Nz) return -1;
   return (long long)(gx - 1) + (long long)(Nx - 1) * ((long long)(gy - 1) + (long long)(Ny - 1) * (gz - 1));
+}
+
+// The same index with the cell's coordinates worked out once (structured_index
+// recomputes them from c on every call): cell_origin gives the grid point of the
+// cell's first node, cell_dof the free index of its tensor position (i, j, k).
+struct CellOrigin {
+  int gx, gy, gz, Nx, Ny, Nz;
+};
+__device__ __forceinline__ CellOrigin cell_origin(long long c, int p, int nx, int ny, int nz) {
+  const int cx = (int)(c % nx);
+  const long long r = c / nx;
+  const int cy = (int)(r % ny);
+  const int cz = (int)(r / ny);
+  return CellOrigin{cx * p, cy * p, cz * p, nx * p, ny * p, nz * p};
+}
+__device__ __forceinline__ long long cell_dof(const CellOrigin& o, int i, int j, int k) {
+  const int gx = o.gx + i, gy = o.gy + j, gz = o.gz + k;
+  if (gx <= 0 || gx >= o.Nx || gy <= 0 || gy >= o.Ny || gz <= 0 || gz >= o.Nz) return -1;
+  return (long long)(gx - 1) +
+         (long long)(o.Nx - 1) * ((long long)(gy - 1) + (long long)(o.Ny - 1) * (gz - 1));
 }
 
 template <typename T>
@@ -109,34 +149,58 @@ __device__ __forceinline__ void stage_mats(const GenParams<SB, SQ, T>& P, T* sMa
 //   backward x  lines (j,k):   U0 = Y = A^T A1 + B^T B1
 // A thread holds at most 2 lines (18 values at Q8) in registers, which keeps
 // several CTAs resident per SM to hide the latency of the per-point metric.
+// Shared copy of the even-odd tables (read with broadcast loads).
 template <int SB, int SQ, typename T>
-__device__ __forceinline__ void line_apply(const T* sMat, const GenParams<SB, SQ, T>& P, int rows,
-                                           int cols, bool transpose, bool useB, T* io, int stride) {
-  // io[r * stride] (r < rows) = sum_c M[r][c] io[c * stride] (c < cols), M = A or B
-  // stored [q][basis]; transpose: M^T. Inputs are read before any output is written.
-  constexpr int N = SB > SQ ? SB : SQ;
-  T in[N];
-  // keeps the compiler from overlapping consecutive line passes (which would
-  // hold several lines in registers at once)
-  asm volatile("" ::: "memory");
+__device__ __forceinline__ void stage_eo(const GenParams<SB, SQ, T>& P, T* sEO) {
+  for (int i = threadIdx.x; i < EOTables<SB, SQ>::TOTAL; i += blockDim.x) sEO[i] = P.eo[i];
+}
+
+// out(r, v) for r < R receives (M u)[r], M one of A, B (OP 0, 1; R = SQ, C = SB) or
+// A^T, B^T (OP 2, 3; R = SB, C = SQ). EO: through the even-odd tables in sEO
+// (about half the FMAs and matrix loads); otherwise the full matrices.
+template <int OP, bool EO, int SB, int SQ, typename T, int R, int C, typename Out>
+__device__ __forceinline__ void contract(const T* sMat, const T* sEO, const GenParams<SB, SQ, T>& P,
+                                         const T (&u)[C], const Out& out) {
+  if constexpr (EO) {
+    using E = EOT<R, C>;
+    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    const V2* tab = reinterpret_cast<const V2*>(sEO + EOTables<SB, SQ>::OFF[OP]);
+    constexpr bool anti = OP == 1 || OP == 3;
+    T ue[E::HC > 0 ? E::HC : 1], uo[E::HC > 0 ? E::HC : 1];
 #pragma unroll
-  for (int c = 0; c < N; ++c)
-    if (c < cols) in[c] = io[c * stride];
-#pragma unroll
-  for (int r = 0; r < N; ++r) {
-    if (r >= rows) break;
-    T acc = T(0);
-#pragma unroll
-    for (int c = 0; c < N; ++c) {
-      if (c >= cols) break;
-      const int ix = transpose ? c * SB + r : r * SB + c;
-      acc = fma(useB ? MB(ix) : MA(ix), in[c], acc);
+    for (int i = 0; i < E::HC; ++i) {
+      ue[i] = u[i] + u[C - 1 - i];
+      uo[i] = u[i] - u[C - 1 - i];
     }
-    io[r * stride] = acc;
+#pragma unroll
+    for (int r = 0; r < E::HR; ++r) {
+      const V2* t = tab + r * (E::W / 2);
+      T e = E::MC ? (T)t[E::HC].x * u[E::HC] : T(0);
+      T o = T(0);
+#pragma unroll
+      for (int i = 0; i < E::HC; ++i) {
+        const V2 eo = t[i];
+        e = fma((T)eo.x, ue[i], e);
+        o = fma((T)eo.y, uo[i], o);
+      }
+      out(r, e + o);
+      if (R - 1 - r != r) out(R - 1 - r, anti ? o - e : e - o);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      T acc = T(0);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int ix = OP < 2 ? r * SB + c : c * SB + r;
+        acc = fma((OP == 0 || OP == 2) ? MA(ix) : MB(ix), u[c], acc);
+      }
+      out(r, acc);
+    }
   }
 }
 
-template <int SB, int SQ, typename T>
+template <int SB, int SQ, typename T, bool EO>
 __global__ void __launch_bounds__(Shape<SB, SQ>::THREADS, Shape<SB, SQ>::MINB)
 k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   using S = Shape<SB, SQ>;
@@ -150,12 +214,27 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   T* U0 = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SL;
   T* U1 = U0 + S::SM3;
   T* U2 = U1 + S::SM3;
-  __shared__ T sMat[kStageMats<T, SB, SQ> ? 2 * SQ * SB : 1];
-  stage_mats<SB, SQ, T>(P, sMat);  // visible after the first __syncthreads below
+  __shared__ T sMat[(!EO && kStageMats<T, SB, SQ>) ? 2 * SQ * SB : 1];
+  __shared__ __align__(16) T sEO[EO ? EOTables<SB, SQ>::TOTAL : 2];
+  if constexpr (EO) stage_eo<SB, SQ, T>(P, sEO);
+  else stage_mats<SB, SQ, T>(P, sMat);  // visible after the first __syncthreads below
   auto at = [](int c3, int c2, int c1) { return (c3 * SM + c2) * SM + c1; };
+  // u[c] = io[c * stride] (c < N); keeps the compiler from overlapping consecutive
+  // line passes, which would hold several lines in registers at once
+  auto load = [](const T* io, int stride, auto& u) {
+    asm volatile("" ::: "memory");
+    constexpr int N = sizeof(u) / sizeof(T);
+#pragma unroll
+    for (int c = 0; c < N; ++c) u[c] = io[c * stride];
+  };
 
   // ---------------- gather ----------------
+  // structured gather only (the table and cell-local modes have no mesh sizes)
+  const CellOrigin org = (valid && !P.ids && P.mode != 1)
+                             ? cell_origin(cell, SB - 1, P.nx, P.ny, P.nz)
+                             : CellOrigin{0, 0, 0, 0, 0, 0};
   for (int pos = l; pos < S::S0; pos += S::NL) {
+    const int i = pos % SB, j = (pos / SB) % SB, k = pos / (SB * SB);
     T v = T(0);
     if (valid) {
       if (P.mode == 1) {
@@ -165,68 +244,66 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
         const int id = P.ids[cell * S::S0 + pos];
         if (id >= 0) v = P.x[id];
       } else {
-        const long long id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+        const long long id = cell_dof(org, i, j, k);
         if (id >= 0) v = P.x[id];
       }
     }
-    const int i = pos % SB, j = (pos / SB) % SB, k = pos / (SB * SB);
     U0[at(k, j, i)] = v;
   }
   __syncthreads();
 
-  // ---------------- forward x: lines (j,k), contract i ----------------
+  // ---------------- forward x: lines (j,k): A1 = A X, B1 = B X ----------------
   if (l < SB * SB) {
     const int j = l % SB, k = l / SB;
-    T in[SB];
-#pragma unroll
-    for (int i = 0; i < SB; ++i) in[i] = U0[at(k, j, i)];
-#pragma unroll
-    for (int qi = 0; qi < SQ; ++qi) {
-      T a = T(0), b = T(0);
-#pragma unroll
-      for (int i = 0; i < SB; ++i) {
-        a = fma(MA(qi * SB + i), in[i], a);
-        b = fma(MB(qi * SB + i), in[i], b);
-      }
-      U1[at(k, j, qi)] = a;
-      U2[at(k, j, qi)] = b;
-    }
+    T u[SB];
+    load(U0 + at(k, j, 0), 1, u);
+    T* a1 = U1 + at(k, j, 0);
+    T* b1 = U2 + at(k, j, 0);
+    contract<0, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { a1[r] = v; });
+    contract<1, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { b1[r] = v; });
   }
   __syncthreads();
 
-  // ---------------- forward y: lines (qi,k), contract j ----------------
+  // ---------- forward y: lines (qi,k): AA = A A1, AB = B A1, BA = A B1 ----------
   if (l < SQ * SB) {
     const int qi = l % SQ, k = l / SQ;
+    T* l0 = U0 + at(k, 0, qi);
+    T* l1 = U1 + at(k, 0, qi);
+    T* l2 = U2 + at(k, 0, qi);
     {
-      T a1[SB];
-#pragma unroll
-      for (int j = 0; j < SB; ++j) a1[j] = U1[at(k, j, qi)];
-#pragma unroll
-      for (int qj = 0; qj < SQ; ++qj) {
-        T aa = T(0), ab = T(0);
-#pragma unroll
-        for (int j = 0; j < SB; ++j) {
-          aa = fma(MA(qj * SB + j), a1[j], aa);
-          ab = fma(MB(qj * SB + j), a1[j], ab);
-        }
-        U1[at(k, qj, qi)] = aa;
-        U0[at(k, qj, qi)] = ab;
-      }
+      T u[SB];
+      load(l1, SM, u);
+      contract<0, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { l1[r * SM] = v; });
+      contract<1, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { l0[r * SM] = v; });
     }
-    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, false, U2 + at(k, 0, qi), SM);  // BA = A B1
+    T u[SB];
+    load(l2, SM, u);
+    contract<0, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { l2[r * SM] = v; });
   }
   __syncthreads();
 
   // ------------- z: forward, metric, backward; lines (qi,qj) -------------
   if (l < SQ * SQ) {
     const int qi = l % SQ, qj = l / SQ;
+    constexpr int ZS = SM * SM;
     T* zx = U2 + at(0, qj, qi);  // BA -> ux -> vx -> back
     T* zy = U0 + at(0, qj, qi);  // AB -> uy -> vy -> back
     T* zz = U1 + at(0, qj, qi);  // AA -> uz -> vz -> back
-    constexpr int ZS = SM * SM;
-    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, false, zx, ZS);
-    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, false, zy, ZS);
-    line_apply<SB, SQ, T>(sMat, P, SQ, SB, false, true, zz, ZS);
+    {
+      T u[SB];
+      load(zx, ZS, u);
+      contract<0, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { zx[r * ZS] = v; });
+    }
+    {
+      T u[SB];
+      load(zy, ZS, u);
+      contract<0, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { zy[r * ZS] = v; });
+    }
+    {
+      T u[SB];
+      load(zz, ZS, u);
+      contract<1, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { zz[r * ZS] = v; });
+    }
     // metric in FP64 (geometric factors are kept in FP64 for both dtypes)
     const double* gt = P.geom == GEOM_SEPARABLE ? nullptr : P.gtab + (valid ? cell : 0) * P.gstride;
 #pragma unroll 3
@@ -252,56 +329,58 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       zy[qk * ZS] = (T)(g[3] * dx + g[1] * dy + g[5] * dz);
       zz[qk * ZS] = (T)(g[4] * dx + g[5] * dy + g[2] * dz);
     }
-    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, false, zx, ZS);
-    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, false, zy, ZS);
-    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, true, zz, ZS);
+    {
+      T u[SQ];
+      load(zx, ZS, u);
+      contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { zx[r * ZS] = v; });
+    }
+    {
+      T u[SQ];
+      load(zy, ZS, u);
+      contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { zy[r * ZS] = v; });
+    }
+    {
+      T u[SQ];
+      load(zz, ZS, u);
+      contract<3, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { zz[r * ZS] = v; });
+    }
   }
   __syncthreads();
 
-  // ---------------- backward y: lines (qi,k), contract qj ----------------
+  // ------- backward y: lines (qi,k): A1 = A^T AA + B^T AB, B1 = A^T BA -------
   if (l < SQ * SB) {
     const int qi = l % SQ, k = l / SQ;
+    T* l0 = U0 + at(k, 0, qi);
+    T* l1 = U1 + at(k, 0, qi);
+    T* l2 = U2 + at(k, 0, qi);
     {
-      T aa[SQ], ab[SQ];
-#pragma unroll
-      for (int qj = 0; qj < SQ; ++qj) {
-        aa[qj] = U1[at(k, qj, qi)];
-        ab[qj] = U0[at(k, qj, qi)];
-      }
-#pragma unroll
-      for (int j = 0; j < SB; ++j) {
-        T a1 = T(0);
-#pragma unroll
-        for (int qj = 0; qj < SQ; ++qj) {
-          a1 = fma(MA(qj * SB + j), aa[qj], a1);
-          a1 = fma(MB(qj * SB + j), ab[qj], a1);
-        }
-        U1[at(k, j, qi)] = a1;
-      }
+      T u[SQ];
+      load(l1, SM, u);
+      contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { l1[r * SM] = v; });
     }
-    line_apply<SB, SQ, T>(sMat, P, SB, SQ, true, false, U2 + at(k, 0, qi), SM);  // B1 = A^T BA
+    {
+      T u[SQ];
+      load(l0, SM, u);
+      contract<3, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { l1[r * SM] += v; });
+    }
+    T u[SQ];
+    load(l2, SM, u);
+    contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { l2[r * SM] = v; });
   }
   __syncthreads();
 
-  // ---------------- backward x: lines (j,k) -> Y in U0 ----------------
+  // ---------------- backward x: lines (j,k): Y = A^T A1 + B^T B1 in U0 ----------------
   if (l < SB * SB) {
     const int j = l % SB, k = l / SB;
-    T a1[SQ], b1[SQ];
-#pragma unroll
-    for (int qi = 0; qi < SQ; ++qi) {
-      a1[qi] = U1[at(k, j, qi)];
-      b1[qi] = U2[at(k, j, qi)];
+    T* y0 = U0 + at(k, j, 0);
+    {
+      T u[SQ];
+      load(U1 + at(k, j, 0), 1, u);
+      contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { y0[r] = v; });
     }
-#pragma unroll
-    for (int i = 0; i < SB; ++i) {
-      T yv = T(0);
-#pragma unroll
-      for (int qi = 0; qi < SQ; ++qi) {
-        yv = fma(MA(qi * SB + i), a1[qi], yv);
-        yv = fma(MB(qi * SB + i), b1[qi], yv);
-      }
-      U0[at(k, j, i)] = yv;
-    }
+    T u[SQ];
+    load(U2 + at(k, j, 0), 1, u);
+    contract<3, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { y0[r] += v; });
   }
   __syncthreads();
 
@@ -316,7 +395,7 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       const int id = P.ids[cell * S::S0 + pos];
       if (id >= 0) atomic_add(P.y + id, v);
     } else {
-      const long long id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+      const long long id = cell_dof(org, i, j, k);
       if (id >= 0) atomic_add(P.y + id, v);
     }
   }
@@ -521,6 +600,24 @@ k_kappa_vjp(const __grid_constant__ GenParams<SB, SQ, T> P, const T* __restrict_
   }
 }
 
+// True when A[SQ-1-q][SB-1-i] = A[q][i] and B[SQ-1-q][SB-1-i] = -B[q][i] (nodes and
+// quadrature points symmetric about the segment's midpoint, which holds for
+// equispaced Lagrange nodes with Gauss points): the even-odd kernel applies.
+bool centro_symmetric(const double* A, const double* B, int SB, int SQ) {
+  double amax = 0.0, bmax = 0.0;
+  for (int i = 0; i < SB * SQ; ++i) {
+    amax = std::fmax(amax, std::fabs(A[i]));
+    bmax = std::fmax(bmax, std::fabs(B[i]));
+  }
+  for (int q = 0; q < SQ; ++q)
+    for (int i = 0; i < SB; ++i) {
+      const int m = (SQ - 1 - q) * SB + (SB - 1 - i);
+      if (std::fabs(A[m] - A[q * SB + i]) > 1e-13 * amax) return false;
+      if (std::fabs(B[m] + B[q * SB + i]) > 1e-13 * bmax) return false;
+    }
+  return true;
+}
+
 template <int SB, int SQ, typename T>
 GenParams<SB, SQ, T> make_params(const double* A, const double* B, const Geometry& geom) {
   GenParams<SB, SQ, T> P{};
@@ -528,6 +625,25 @@ GenParams<SB, SQ, T> make_params(const double* A, const double* B, const Geometr
     P.A[i] = (T)A[i];
     P.B[i] = (T)B[i];
   }
+  // even-odd tables of A, B, A^T, B^T (see EOT)
+  auto fill = [&](int op, int R, int C, auto m) {
+    const int HR = (R + 1) / 2, HC = C / 2, MC = C % 2, W = 2 * HC + 2 * MC;
+    T* t = P.eo + EOTables<SB, SQ>::OFF[op];
+    for (int r = 0; r < HR; ++r) {
+      for (int i = 0; i < HC; ++i) {
+        t[r * W + 2 * i] = (T)(0.5 * (m(r, i) + m(r, C - 1 - i)));
+        t[r * W + 2 * i + 1] = (T)(0.5 * (m(r, i) - m(r, C - 1 - i)));
+      }
+      if (MC) {
+        t[r * W + 2 * HC] = (T)m(r, HC);
+        t[r * W + 2 * HC + 1] = T(0);
+      }
+    }
+  };
+  fill(0, SQ, SB, [&](int r, int c) { return A[r * SB + c]; });
+  fill(1, SQ, SB, [&](int r, int c) { return B[r * SB + c]; });
+  fill(2, SB, SQ, [&](int r, int c) { return A[c * SB + r]; });
+  fill(3, SB, SQ, [&](int r, int c) { return B[c * SB + r]; });
   for (int i = 0; i < SQ; ++i) P.w1[i] = geom.w1[i];
   for (int c = 0; c < 6; ++c) P.G0[c] = geom.G0[c];
   P.geom = geom.kind;
@@ -562,11 +678,12 @@ void run_general(int mode, const double* A, const double* B, const Cells& cells,
     return;
   }
   const size_t smem = (size_t)S::EPB * S::SL * sizeof(T);
-  SF_CUDA_CHECK(cudaFuncSetAttribute(k_general<SB, SQ, T>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long blocks = (ncells + S::EPB - 1) / S::EPB;
   SF_REQUIRE(blocks < (1LL << 31), SF_ERR_ARG, "too many cells for one launch");
-  k_general<SB, SQ, T><<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
+  auto kern = centro_symmetric(A, B, SB, SQ) ? k_general<SB, SQ, T, true>
+                                             : k_general<SB, SQ, T, false>;
+  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
