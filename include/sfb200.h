@@ -94,6 +94,27 @@ int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* 
 int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_order);
 
 /*
+ * The z-slab of cells [z0, z1) of an nx x ny x nz structured mesh (the share of
+ * one rank when the mesh is split along z; the reference's Gridap model is one
+ * process, so this has no single counterpart there). Vectors of a slab
+ * operator hold the free points of the grid z-levels z0 p .. (z1 + 1) p, level
+ * by level (plane_size = (nx p - 1)(ny p - 1) points each, x fastest):
+ *   plane 0              halo: level z0 p, owned by the rank below (or the
+ *                        Dirichlet boundary, then zero);
+ *   planes 1 .. (z1-z0)p owned: levels z0 p + 1 .. z1 p, except that level nz p
+ *                        (the top boundary, z1 = nz) is Dirichlet and stays zero;
+ *   the last p planes    halo: levels z1 p + 1 .. (z1 + 1) p, owned by the rank
+ *                        above (zero past the top of the mesh).
+ * n_free is the whole slab vector. sf_apply reads all planes and writes the
+ * owned points only; sf_diagonal (FP64) writes diag(A) at the owned points.
+ * The slab must use the tiled Cartesian kernel (axis-aligned affine cells,
+ * constant coefficient). sf_get_info "owned_offset" / "owned_count" give the
+ * owned range.
+ */
+int sf_set_structured_slab(sf_op* op, int nx, int ny, int nz, int z0, int z1,
+                           const int32_t* node_order);
+
+/*
  * Geometric factors at the quadrature points, exactly the triple
  * (cell_wq, cell_jq, cell_djq) of LazyMatrix (src/LazyMatrices.jl:34-43):
  *   wq  : SQ^D weights per cell (linear qp index, i1 fastest)
@@ -166,6 +187,39 @@ int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int ma
           int* iters, double* relres, void* stream);
 
 /*
+ * Jacobi FP64 CG in steps, for an operator split over ranks (slab operators;
+ * a full operator works too, as one rank). The distributed form of
+ * IterativeSolvers.cg! (profiling/drivers.jl:85-95). The caller owns the
+ * vectors (all n_free long, slab layout) and a device block s of
+ * SF_CGD_SCALARS doubles. It keeps the halo planes of x (before sf_cgd_start)
+ * and of p (before each sf_cgd_apply) current, and after the steps marked
+ * "sum" adds the listed entries of s over all ranks in place (e.g. an NCCL
+ * all-reduce). One solve:
+ *   sf_cgd_start(b, x, r, p, q, s)       r = b - A x, p = D^-1 r   sum s[2..4]
+ *   sf_cgd_init(s, reltol)
+ *   repeat:  exchange p halos
+ *            sf_cgd_apply(p, q, s)       q = A p                   sum s[10]
+ *            sf_cgd_update(r, q, s)      r -= alpha q              sum s[11..12]
+ *            sf_cgd_direction(x, p, r, s) x += alpha p, p = D^-1 r + beta p
+ * until s[SF_CGD_DONE] != 0 (read it every few iterations: steps after the
+ * converged one change nothing, so every rank can run the same steps).
+ * s[SF_CGD_DONE]: 0 running, 2 converged (relres <= reltol), 3 non-finite
+ * residual. s[SF_CGD_ITERS] iterations; s[SF_CGD_RR] and s[SF_CGD_BB] the
+ * summed squared norms of r and b.
+ */
+#define SF_CGD_SCALARS 16
+#define SF_CGD_RR 3
+#define SF_CGD_BB 4
+#define SF_CGD_DONE 5
+#define SF_CGD_ITERS 6
+int sf_cgd_start(sf_op* op, const double* b, const double* x, double* r, double* p, double* q,
+                 double* s, void* stream);
+int sf_cgd_init(sf_op* op, double* s, double reltol, void* stream);
+int sf_cgd_apply(sf_op* op, const double* p, double* q, double* s, void* stream);
+int sf_cgd_update(sf_op* op, double* r, const double* q, double* s, void* stream);
+int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s, void* stream);
+
+/*
  * Named numeric options of a handle:
  *   "mixed_inner_reltol" : SF_CG_MIXED refines (FP64 true residual replaces the FP32
  *                          recurrence residual) each time the FP32 residual has
@@ -185,6 +239,10 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *   "kernels_per_apply"      : kernel launches one sf_apply(SF_F64) makes
  *   "geometry_kind"          : 1 separable constant metric, 2 per-point table
  *   "tile_candidates_f64/f32": number of tile shapes of the tiled kernel (0 if not in use)
+ *   "slab"                   : 1 for a slab operator (sf_set_structured_slab)
+ *   "plane_size"             : free points per z-level (structured meshes)
+ *   "owned_offset", "owned_count": the points sf_apply writes (the whole vector
+ *                              unless the operator is a slab)
  */
 int sf_get_info(const sf_op* op, const char* key, double* value);
 

@@ -11,12 +11,12 @@ from . import fem
 from ._lib import LIB_PATH, SumFacError
 from .fem import (CartesianDiscreteModel, FESpace, Measure, Table, TrialFESpace,
                   cell_quantities)
-from . import adjoint, batch
+from . import adjoint, batch, distributed
 from .operator import (LazyMatrix, SumFactorizationMap, assemble_rhs, cg, get_dimensional_parameters,
                        mul, mul_multi)
 
 __all__ = [
     "CartesianDiscreteModel", "FESpace", "TrialFESpace", "Measure", "Table", "cell_quantities",
     "SumFactorizationMap", "get_dimensional_parameters", "LazyMatrix", "mul", "mul_multi", "cg",
-    "assemble_rhs", "SumFacError", "LIB_PATH", "fem", "adjoint", "batch",
+    "assemble_rhs", "SumFacError", "LIB_PATH", "fem", "adjoint", "batch", "distributed",
 ]

@@ -73,9 +73,21 @@ SIGNATURES = {
     "sf_batch_autotune": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), vp]),
     "sf_batch_group_kernel": (C.c_char_p, [vp, i32, i32]),
     "sf_kernel_name": (C.c_char_p, [vp, i32]),
+    "sf_set_structured_slab": (i32, [vp, i32, i32, i32, i32, i32, vp]),
+    "sf_cgd_start": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "sf_cgd_init": (i32, [vp, vp, C.c_double, vp]),
+    "sf_cgd_apply": (i32, [vp, vp, vp, vp, vp]),
+    "sf_cgd_update": (i32, [vp, vp, vp, vp, vp]),
+    "sf_cgd_direction": (i32, [vp, vp, vp, vp, vp, vp]),
 }
 
 SF_NOALLOC_MAX_FREE = 262144
+
+SF_CGD_SCALARS = 16
+SF_CGD_RR = 3
+SF_CGD_BB = 4
+SF_CGD_DONE = 5
+SF_CGD_ITERS = 6
 
 for _name, (_res, _args) in SIGNATURES.items():
     _f = getattr(lib, _name)

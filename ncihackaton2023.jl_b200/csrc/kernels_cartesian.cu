@@ -36,6 +36,7 @@
 // is written back coalesced.
 #include "sf_cartesian.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -65,7 +66,8 @@ struct CartParams {
   T rz, rx, cy;                    // cz/cy, cx/cy, cy
   const T* x;
   T* y;
-  int nfx, nfy, nfz;  // free grid
+  int nfx, nfy, nfz;  // free grid (inputs are read for z in [zlo, nfz))
+  int zlo, nfz_out;   // lowest input z (-1 on a slab: the halo plane below); outputs z < nfz_out
   int ntx, nty, ntz;  // tiles
   double* dot;  // non-null: dot[tile] = sum of x*y over the tile's outputs
 };
@@ -247,14 +249,17 @@ __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body&
 }
 
 // One output tile: cells [tx*EX, (tx+1)*EX) x [ty*EY, ...) x [tz*EZ, ...) of a free grid
-// nfx x nfy x nfz. T1/T2: shared buffers of Tile::TS words each. Ends with the
+// nfx x nfy x nfz. Inputs outside the free grid read as zero, except that the
+// z range read is [zlo, nfz) (zlo = -1: a slab's halo plane below it); outputs
+// are written for z < nfz_out. T1/T2: shared buffers of Tile::TS words each. Ends with the
 // outputs stored; the caller synchronises before reusing T1/T2. With `dot`
 // non-null, *dot receives the FP64 sum of x*y over the tile's outputs (the
 // (p, A p) term of CG), summed in a fixed order.
 template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T>
 __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
                                           const EOMat<P, T>& Km, const T* __restrict__ X,
-                                          T* __restrict__ Y, int nfx, int nfy, int nfz, int tx,
+                                          T* __restrict__ Y, int nfx, int nfy, int nfz, int zlo,
+                                          int nfz_out, int tx,
                                           int ty, int tz, T rz, T rx, T cy,
                                           double* dot = nullptr) {
   using G = Tile<P, EX, EY, EZ, T>;
@@ -263,7 +268,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   const long long pz = (long long)nfx * nfy;
 
   // a tile whose whole input box lies inside the free grid needs no bounds checks
-  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= 0 && fx0 + G::BX <= nfx &&
+  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= zlo && fx0 + G::BX <= nfx &&
                         fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
 
   // ---- z pass: one z-line per thread, read from global memory ----
@@ -280,7 +285,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
 #pragma unroll
       for (int z = 0; z < G::BZ; ++z) {
         const int fz = fz0 + z;
-        c[z] = (inxy && (unsigned)fz < (unsigned)nfz) ? __ldg(col + fz * pz) : T(0);
+        c[z] = (inxy && (unsigned)(fz - zlo) < (unsigned)(nfz - zlo)) ? __ldg(col + fz * pz) : T(0);
       }
     }
   };
@@ -375,7 +380,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
 
   // ---- store the owned outputs (free coords start at e0*p) ----
   const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
-  const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz;
+  const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz_out;
   const long long base = (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
   T* ybase = Y + base;
   constexpr int NOUT = G::OX * G::OY * G::OZ;
@@ -386,7 +391,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     const int zo = r / G::OY;
     o = xo + (long long)nfx * (yo + (long long)nfy * zo);
     t1 = zo * G::PLANE + yo * G::BX + xo;
-    return full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz);
+    return full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz_out);
   };
   if (!dot) {
     for (int i = threadIdx.x; i < NOUT; i += NT) {
@@ -433,10 +438,41 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   Mm.load(Q.Me, Q.Mo);
   Km.load(Q.Ke, Q.Ko);
   const int tile = blockIdx.x;
-  cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz,
+  cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz, Q.zlo,
+                                       Q.nfz_out,
                                        tile % Q.ntx, (tile / Q.ntx) % Q.nty,
                                        tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy,
                                        Q.dot ? Q.dot + tile : nullptr);
+}
+
+// diag(A) on the free points written by an apply (full mesh or slab). On a
+// Cartesian mesh A = cx Kx(x)My(x)Mz + cy Mx(x)Ky(x)Mz + cz Mx(x)My(x)Kz with the 1D
+// operators assembled along each axis, so diag(A) is the same sum of products
+// of the assembled 1D diagonals: K[l][l] at a cell-interior node l, and
+// K[0][0] + K[p][p] at a vertex (every free vertex lies between two cells).
+struct DiagParams {
+  double Kd[kMaxSB], Md[kMaxSB];
+  double c[3];
+  double* d;  // first written point
+  int p, nfx, nfy, nfz_out;
+};
+
+__global__ void k_cartesian_diag(const __grid_constant__ DiagParams Q) {
+  const long long n = (long long)Q.nfx * Q.nfy * Q.nfz_out;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int gx = (int)(i % Q.nfx) + 1;
+    const long long r = i / Q.nfx;
+    const int gy = (int)(r % Q.nfy) + 1;
+    const int gz = (int)(r / Q.nfy) + 1;  // grid level, modulo p (a slab starts on a vertex)
+    auto d1 = [&](const double* D, int g) {
+      const int l = g % Q.p;
+      return l == 0 ? D[0] + D[Q.p] : D[l];
+    };
+    Q.d[i] = Q.c[0] * d1(Q.Kd, gx) * d1(Q.Md, gy) * d1(Q.Md, gz) +
+             Q.c[1] * d1(Q.Md, gx) * d1(Q.Kd, gy) * d1(Q.Md, gz) +
+             Q.c[2] * d1(Q.Md, gx) * d1(Q.Md, gy) * d1(Q.Kd, gz);
+  }
 }
 
 template <int P, typename T>
@@ -510,7 +546,7 @@ k_cartesian_batch(const __grid_constant__ BatchParams<P, T> Q) {
     const long long rhs = local / tiles;
     const int tile = (int)(local - rhs * tiles);
     cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, pb.x + rhs * pb.ldx, pb.y + rhs * pb.ldy,
-                                         pb.nfx, pb.nfy, pb.nfz, tile % pb.ntx,
+                                         pb.nfx, pb.nfy, pb.nfz, 0, pb.nfz, tile % pb.ntx,
                                          (tile / pb.ntx) % pb.nty, tile / (pb.ntx * pb.nty),
                                          pb.rz, pb.rx, pb.cy);
     __syncthreads();  // T1/T2 and s_item are reused by the next item
@@ -561,6 +597,16 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   Q.nfx = plan.nx * P - 1;
   Q.nfy = plan.ny * P - 1;
   Q.nfz = plan.nz * P - 1;
+  Q.zlo = 0;
+  Q.nfz_out = Q.nfz;
+  if (plan.slab) {  // planes of levels z0 p .. (z1 + 1) p; outputs on levels z0 p + 1 ..
+    const long long pz = (long long)Q.nfx * Q.nfy;
+    Q.x += pz;
+    Q.y += pz;
+    Q.nfz = (plan.nz + 1) * P;
+    Q.zlo = -1;
+    Q.nfz_out = plan.nz * P - (plan.slab_top ? 1 : 0);
+  }
   Q.ntx = (plan.nx + EX - 1) / EX;
   Q.nty = (plan.ny + EY - 1) / EY;
   Q.ntz = (plan.nz + EZ - 1) / EZ;
@@ -740,6 +786,27 @@ void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* 
                      cudaStream_t stream, const CartFuse& fuse) {
   SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
   pick(plan, dtype, plan.choice[dtype_slot(dtype)]).run(plan, x, y, fuse, stream);
+}
+
+void cartesian_diag(const CartesianPlan& plan, double* d, cudaStream_t stream) {
+  SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
+  DiagParams Q{};
+  const int SB = plan.SB, P = SB - 1;
+  for (int l = 0; l < SB; ++l) {
+    Q.Kd[l] = plan.K[l * SB + l];
+    Q.Md[l] = plan.M[l * SB + l];
+  }
+  for (int k = 0; k < 3; ++k) Q.c[k] = plan.c[k];
+  Q.p = P;
+  Q.nfx = plan.nx * P - 1;
+  Q.nfy = plan.ny * P - 1;
+  Q.nfz_out = plan.slab ? plan.nz * P - (plan.slab_top ? 1 : 0) : plan.nz * P - 1;
+  Q.d = d + (plan.slab ? (long long)Q.nfx * Q.nfy : 0);
+  const long long n = (long long)Q.nfx * Q.nfy * Q.nfz_out;
+  if (n <= 0) return;
+  const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 16);
+  k_cartesian_diag<<<(unsigned)blocks, 256, 0, stream>>>(Q);
+  SF_CUDA_CHECK(cudaGetLastError());
 }
 
 long long cartesian_tiles(const CartesianPlan& plan, int dtype) {

@@ -173,9 +173,10 @@ __global__ void k_cg_init(double* __restrict__ s, double reltol2) {
 template <typename T>
 __global__ void k_cg_update(double* __restrict__ s, T* __restrict__ r, const T* __restrict__ q,
                             const T* __restrict__ dinv, long long n,
-                            double* __restrict__ partials) {
+                            double* __restrict__ partials, int distributed) {
   if (s[CG_DONE] != 0.0) return;
-  const T alpha = (T)(s[CG_RZ] / s[CG_PQ]);
+  const double pq = distributed ? s[CG_PART_PQ] : s[CG_PQ];
+  const T alpha = (T)(s[CG_RZ] / pq);
   const long long S = (long long)gridDim.x * kThreads;
   long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
   double v[2] = {0.0, 0.0};
@@ -204,11 +205,27 @@ __global__ void k_cg_update(double* __restrict__ s, T* __restrict__ r, const T* 
     v[1] += (double)ri * (double)ri;
   }
   if (last_block_sum<2>(v, partials, cg_counter(s)) && threadIdx.x == 0) {
-    s[CG_RZ_NEW] = v[0];
-    s[CG_RR] = v[1];
-    if (!isfinite(v[1]) || !isfinite(v[0])) s[CG_DONE] = 3.0;
-    else if (v[1] <= s[CG_TOL2]) s[CG_DONE] = 1.0;
+    if (distributed) {
+      s[CG_PQ] = pq;
+      s[CG_PART_RZ] = v[0];
+      s[CG_PART_RR] = v[1];
+    } else {
+      s[CG_RZ_NEW] = v[0];
+      s[CG_RR] = v[1];
+      if (!isfinite(v[1]) || !isfinite(v[0])) s[CG_DONE] = 3.0;
+      else if (v[1] <= s[CG_TOL2]) s[CG_DONE] = 1.0;
+    }
   }
+}
+
+// distributed CG: the summed (r, dinv r) and (r, r), and the stopping test
+__global__ void k_cg_check(double* __restrict__ s) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || s[CG_DONE] != 0.0) return;
+  const double rz = s[CG_PART_RZ], rr = s[CG_PART_RR];
+  s[CG_RZ_NEW] = rz;
+  s[CG_RR] = rr;
+  if (!isfinite(rr) || !isfinite(rz)) s[CG_DONE] = 3.0;
+  else if (rr <= s[CG_TOL2]) s[CG_DONE] = 1.0;
 }
 
 // x += alpha p; then p = dinv r + beta p unless this iteration converged. The
@@ -378,8 +395,14 @@ void cg_init(double* s, double reltol2, cudaStream_t st) {
 
 template <typename T>
 void cg_update(double* s, T* r, const T* q, const T* dinv, long long n, double* partials,
-               cudaStream_t st) {
-  k_cg_update<T><<<grid_for(k_cg_update<T>, n), kThreads, 0, st>>>(s, r, q, dinv, n, partials);
+               cudaStream_t st, bool distributed) {
+  k_cg_update<T><<<grid_for(k_cg_update<T>, n), kThreads, 0, st>>>(s, r, q, dinv, n, partials,
+                                                                   distributed ? 1 : 0);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+void cg_check(double* s, cudaStream_t st) {
+  k_cg_check<<<1, 32, 0, st>>>(s);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -420,7 +443,8 @@ void copy_scalar(double* s, int dst, int src, cudaStream_t st) {
                            const double*, cudaStream_t);                                        \
   template void cg_start<T>(const T*, const T*, const T*, T*, T*, long long, double*, double*,  \
                             cudaStream_t);                                                      \
-  template void cg_update<T>(double*, T*, const T*, const T*, long long, double*, cudaStream_t); \
+  template void cg_update<T>(double*, T*, const T*, const T*, long long, double*, cudaStream_t,  \
+                             bool);                                                             \
   template void cg_direction<T>(double*, T*, T*, const T*, const T*, long long, double*,        \
                                 cudaStream_t);                                                  \
   template void vec_invert<T>(const double*, T*, long long, cudaStream_t);

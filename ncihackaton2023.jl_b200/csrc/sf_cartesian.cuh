@@ -13,6 +13,10 @@ struct CartesianPlan {
   double K[kMaxSB * kMaxSB] = {0};  // 1D element stiffness B^T W B
   double c[3] = {0, 0, 0};          // G0 diagonal: xx, yy, zz
   int choice[2] = {0, 0};           // tile candidate per dtype (0: FP64, 1: FP32)
+  // z-slab of a larger mesh: nz cells of it; vectors hold the grid levels z0 p .. (z0 + nz + 1) p
+  // (one halo plane below, p above); outputs on levels z0 p + 1 .. (z0 + nz) p, the last one
+  // left out when it is the mesh's Dirichlet boundary (slab_top)
+  bool slab = false, slab_top = false;
 };
 
 // Optional work fused into one apply of the CG loop.
@@ -45,6 +49,8 @@ void cartesian_batch_launch(const CartesianPlan& proto, int dtype, int cand, con
                             cudaStream_t st);
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
                      cudaStream_t stream, const CartFuse& fuse = CartFuse{});
+// diag(A) at the points an apply writes (same layout as y; other points untouched).
+void cartesian_diag(const CartesianPlan& plan, double* d, cudaStream_t stream);
 // Tiles (CTAs) of one apply with the chosen candidate: the entries CartFuse::dot receives.
 long long cartesian_tiles(const CartesianPlan& plan, int dtype);
 void cartesian_release(CartesianPlan& plan);

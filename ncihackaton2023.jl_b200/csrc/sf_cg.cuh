@@ -15,8 +15,11 @@ enum CgSlot {
   CG_DONE = 5,    // 0 running; 1 converged by this iteration's update; 2 finished; 3 non-finite
   CG_ITERS = 6,   // completed iterations
   CG_TOL2 = 7,    // stopping threshold on (r, r); negative: never stop on the device
-  CG_REPORTS = 8,  // direction steps run since cg_init (the number of the last report)
-  CG_COUNTER = 9,  // storage of the unsigned block counter of the last-block reductions
+  CG_REPORTS = 8,   // direction steps run since cg_init (the number of the last report)
+  CG_COUNTER = 9,   // storage of the unsigned block counter of the last-block reductions
+  CG_PART_PQ = 10,  // distributed CG: this rank's (p, q), then (after the caller's sum) all ranks'
+  CG_PART_RZ = 11,  // distributed CG: (r, dinv r), likewise
+  CG_PART_RR = 12,  // distributed CG: (r, r), likewise
   CG_NSLOTS = 16
 };
 
@@ -51,9 +54,13 @@ void cg_start(const T* b, const T* q, const T* dinv, T* r, T* p, long long n, do
 // After cg_start or mixed_residual: RZ = RZ_NEW, ITERS = 0, TOL2 = reltol2 * max(BB, 1 if
 // BB = 0) (or -1 for reltol2 < 0), DONE = 2 if RR <= TOL2 already (3 if RR is not finite).
 void cg_init(double* s, double reltol2, cudaStream_t st);
+// distributed: alpha = RZ / s[PART_PQ] (then PQ = PART_PQ), sums into PART_RZ, PART_RR and
+// no stopping test (cg_check does it once the caller has summed them over ranks)
 template <typename T>
 void cg_update(double* s, T* r, const T* q, const T* dinv, long long n, double* partials,
-               cudaStream_t st);
+               cudaStream_t st, bool distributed = false);
+// distributed: RZ_NEW = PART_RZ, RR = PART_RR and the stopping test (nothing once DONE != 0)
+void cg_check(double* s, cudaStream_t st);
 template <typename T>
 void cg_direction(double* s, T* x, T* p, const T* r, const T* dinv, long long n, double* report,
                   cudaStream_t st);

@@ -38,6 +38,11 @@ struct sf_op {
   long long cq_cells = -1;  // -1 = unset, 0 = fill (one cell for all)
   bool cartesian_ok = false;
   sf::CartesianPlan cart;   // tiled Cartesian kernel set-up
+  // z-slab of a structured mesh (sf_set_structured_slab): cells [slab_z0, slab_z1) of mesh_nz
+  bool slab = false;
+  int slab_z0 = 0, slab_z1 = 0, mesh_nz = 0;
+  long long plane = 0;       // free points per z level
+  double* d_dinv = nullptr;  // 1 / diag(A) on the owned points (distributed CG)
   // workspaces
   double* d_diag = nullptr;  // FP64 diag(A), cached
   void* d_ws = nullptr;
@@ -145,6 +150,8 @@ void update_cartesian(sf_op* op) {
   op->cartesian_ok = sf::cartesian_prepare(op->cart, op->SB, op->SQ, op->A.data(), op->B.data(),
                                            op->geom.w1, G, op->cells.nx, op->cells.ny,
                                            op->cells.nz);
+  op->cart.slab = op->slab;
+  op->cart.slab_top = op->slab && op->slab_z1 == op->mesh_nz;
 }
 
 void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
@@ -157,22 +164,59 @@ void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
     sf::cartesian_apply(op->cart, dtype, x, y, st);
     return;
   }
+  SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED,
+             "a slab operator needs the tiled Cartesian kernel (axis-aligned affine cells, "
+             "constant coefficient)");
   SF_CUDA_CHECK(cudaMemsetAsync(y, 0, op->n_free * es, st));
   sf::launch_general_apply(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
                            x, y, st);
 }
 
+// diag(A) into d (n_free FP64, zeroed first): the Kronecker form on Cartesian
+// operators, the element kernel otherwise.
+void compute_diag(sf_op* op, double* d, cudaStream_t st) {
+  SF_CUDA_CHECK(cudaMemsetAsync(d, 0, op->n_free * sizeof(double), st));
+  if (op->cartesian_ok) {
+    sf::cartesian_diag(op->cart, d, st);
+    return;
+  }
+  SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "a slab operator needs the tiled Cartesian kernel");
+  sf::launch_general_diag(SF_F64, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
+                          d, st);
+}
+
 void ensure_diag(sf_op* op, cudaStream_t st) {
   if (op->d_diag) return;
   op->d_diag = dalloc<double>(op->n_free);
-  SF_CUDA_CHECK(cudaMemsetAsync(op->d_diag, 0, op->n_free * sizeof(double), st));
-  sf::launch_general_diag(SF_F64, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
-                          op->d_diag, st);
+  compute_diag(op, op->d_diag, st);
+}
+
+// The points a slab operator owns: the planes after the lower halo plane, up to
+// the upper halo (the top plane left out when it is the Dirichlet boundary).
+long long owned_offset(const sf_op* op) { return op->slab ? op->plane : 0; }
+long long owned_count(const sf_op* op) {
+  if (!op->slab) return op->n_free;
+  const long long planes = (long long)(op->slab_z1 - op->slab_z0) * op->p -
+                           (op->slab_z1 == op->mesh_nz ? 1 : 0);
+  return planes * op->plane;
+}
+
+// 1 / diag(A) on the owned points (zero elsewhere), cached.
+const double* ensure_dinv(sf_op* op, cudaStream_t st) {
+  if (op->d_dinv) return op->d_dinv;
+  ensure_diag(op, st);
+  op->d_dinv = dalloc<double>(op->n_free);
+  SF_CUDA_CHECK(cudaMemsetAsync(op->d_dinv, 0, op->n_free * sizeof(double), st));
+  const long long off = owned_offset(op);
+  sf::vec_invert<double>(op->d_diag + off, op->d_dinv + off, owned_count(op), st);
+  return op->d_dinv;
 }
 
 void invalidate_caches(sf_op* op) {
   dfree(op->d_diag);
   op->d_diag = nullptr;
+  dfree(op->d_dinv);
+  op->d_dinv = nullptr;
 }
 
 void* workspace(sf_op* op, size_t bytes) {
@@ -462,6 +506,7 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_gtab);
   dfree(op->d_kappa);
   dfree(op->d_diag);
+  dfree(op->d_dinv);
   dfree(op->d_ws);
   dfree(op->d_hx);
   dfree(op->d_hy);
@@ -548,6 +593,28 @@ int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_ord
     op->cells.nz = nz;
     op->cells.p = op->p;
     op->n_free = fx * fy * fz;
+    op->slab = false;
+    op->plane = fx * fy;
+    invalidate_caches(op);
+    update_cartesian(op);
+  });
+}
+
+int sf_set_structured_slab(sf_op* op, int nx, int ny, int nz, int z0, int z1,
+                           const int32_t* node_order) {
+  if (!op) return SF_ERR_ARG;
+  const int status = sf_set_structured(op, nx, ny, z1 > z0 ? z1 - z0 : 1, node_order);
+  if (status != SF_OK) return status;
+  return guarded(op, [&] {
+    SF_REQUIRE(nz > 0 && z0 >= 0 && z0 < z1 && z1 <= nz, SF_ERR_ARG,
+               "slab cells [z0, z1) must lie in [0, nz) and be non-empty");
+    const long long p = op->p;
+    op->slab = true;
+    op->slab_z0 = z0;
+    op->slab_z1 = z1;
+    op->mesh_nz = nz;
+    op->n_free = op->plane * ((long long)(z1 - z0 + 1) * p + 1);
+    SF_REQUIRE(op->n_free < (1LL << 31), SF_ERR_ARG, "slab too large for int32 dof ids");
     invalidate_caches(op);
     update_cartesian(op);
   });
@@ -675,6 +742,7 @@ int sf_kappa_vjp(sf_op* op, int dtype, const void* x, const void* ybar, double* 
   if (!op) return SF_ERR_ARG;
   return guarded(op, [&] {
     require_ready(op);
+    SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_kappa_vjp does not take slab operators");
     SF_REQUIRE(x && ybar && kappa_bar, SF_ERR_ARG, "null x, ybar or kappa_bar");
     sf::launch_kappa_vjp(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, x,
                          ybar, kappa_bar, static_cast<cudaStream_t>(stream));
@@ -742,6 +810,11 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream) {
     SF_REQUIRE(d, SF_ERR_ARG, "null d");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t es = dsize(dtype);
+    if (op->slab) {
+      SF_REQUIRE(dtype == SF_F64, SF_ERR_UNSUPPORTED, "the diagonal of a slab operator is FP64");
+      compute_diag(op, static_cast<double*>(d), st);
+      return;
+    }
     SF_CUDA_CHECK(cudaMemsetAsync(d, 0, op->n_free * es, st));
     sf::launch_general_diag(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
                             d, st);
@@ -753,6 +826,8 @@ int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int ma
   if (!op) return SF_ERR_ARG;
   int status = guarded(op, [&] {
     require_ready(op);
+    SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED,
+               "a slab operator solves through the distributed CG steps (sf_cgd_*)");
     SF_REQUIRE(b && x, SF_ERR_ARG, "null b or x");
     SF_REQUIRE(reltol > 0 && maxiter >= 0, SF_ERR_ARG, "bad reltol / maxiter");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -772,6 +847,84 @@ int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int ma
     if (!(rel <= reltol)) throw Error(SF_ERR_NOT_CONVERGED, "CG reached its iteration cap");
   });
   return status;
+}
+
+// ---------------------------------------------------------------------------
+// Distributed Jacobi CG in steps (slab operators; also a single full operator).
+// The caller owns the slab-layout vectors and the scalar block s, exchanges
+// the halo planes of x (before sf_cgd_start) and of p (before each
+// sf_cgd_apply), and sums the listed entries of s over the ranks in place
+// between the steps. Every kernel here works on the owned points only, except
+// the apply, which reads the halo planes.
+// ---------------------------------------------------------------------------
+int sf_cgd_start(sf_op* op, const double* b, const double* x, double* r, double* p, double* q,
+                 double* s, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(b && x && r && p && q && s, SF_ERR_ARG, "null vector or scalar block");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long off = owned_offset(op), n = owned_count(op);
+    const double* dinv = ensure_dinv(op, st);
+    double* partials = static_cast<double*>(workspace(op, cg_partials(op) * sizeof(double)));
+    sf::cg_reset(s, st);
+    apply_impl(op, SF_F64, x, q, st);
+    sf::cg_start<double>(b + off, q + off, dinv + off, r + off, p + off, n, partials, s, st);
+  });
+}
+
+int sf_cgd_init(sf_op* op, double* s, double reltol, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    SF_REQUIRE(s && reltol > 0, SF_ERR_ARG, "null scalar block or bad reltol");
+    sf::cg_init(s, reltol * reltol, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int sf_cgd_apply(sf_op* op, const double* p, double* q, double* s, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(p && q && s, SF_ERR_ARG, "null p, q or scalar block");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* partials = static_cast<double*>(workspace(op, cg_partials(op) * sizeof(double)));
+    if (tiled(op, SF_F64)) {
+      sf::CartFuse fuse;
+      fuse.dot = partials;
+      sf::cartesian_apply(op->cart, SF_F64, p, q, st, fuse);
+      sf::dot_finish(partials, sf::cartesian_tiles(op->cart, SF_F64), s + sf::CG_PART_PQ,
+                     s + sf::CG_DONE, st);
+    } else {
+      apply_impl(op, SF_F64, p, q, st);
+      sf::vec_dot<double>(p, q, op->n_free, partials, s + sf::CG_PART_PQ, s, s + sf::CG_DONE, st);
+    }
+  });
+}
+
+int sf_cgd_update(sf_op* op, double* r, const double* q, double* s, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(r && q && s, SF_ERR_ARG, "null r, q or scalar block");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long off = owned_offset(op), n = owned_count(op);
+    const double* dinv = ensure_dinv(op, st);
+    double* partials = static_cast<double*>(workspace(op, cg_partials(op) * sizeof(double)));
+    sf::cg_update<double>(s, r + off, q + off, dinv + off, n, partials, st, true);
+  });
+}
+
+int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(x && p && r && s, SF_ERR_ARG, "null x, p, r or scalar block");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long off = owned_offset(op), n = owned_count(op);
+    const double* dinv = ensure_dinv(op, st);
+    sf::cg_check(s, st);
+    sf::cg_direction<double>(s, x + off, p + off, r + off, dinv + off, n, nullptr, st);
+  });
 }
 
 int sf_set_option(sf_op* op, const char* name, double value) {
@@ -859,6 +1012,10 @@ int sf_get_info(const sf_op* op, const char* key, double* value) {
   else if (k == "tiled_kernel") *value = tiled ? 1.0 : 0.0;
   else if (k == "kernels_per_apply") *value = tiled ? (double)sf::cartesian_launches(op->cart) : 1.0;
   else if (k == "geometry_kind") *value = (double)op->geom.kind;
+  else if (k == "slab") *value = op->slab ? 1.0 : 0.0;
+  else if (k == "plane_size") *value = (double)op->plane;
+  else if (k == "owned_offset") *value = (double)owned_offset(op);
+  else if (k == "owned_count") *value = (double)owned_count(op);
   else if (k == "tile_candidates_f64" || k == "tile_candidates_f32") {
     const int dt = k == "tile_candidates_f64" ? SF_F64 : SF_F32;
     *value = (op->cartesian_ok && sf::cartesian_supported(op->cart, dt))
@@ -949,9 +1106,7 @@ int cg_f64_noalloc(sf_op* op, bool jacobi, const double* b, double* x, double re
   double* s = base + 5 * kNoAllocMaxFree;
   double* partials = s + kNoAllocScalarWords;
   if (jacobi) {
-    SF_CUDA_CHECK(cudaMemsetAsync(diag, 0, n * sizeof(double), st));
-    sf::launch_general_diag(SF_F64, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells,
-                            op->geom, diag, st);
+    compute_diag(op, diag, st);
     sf::vec_invert<double>(diag, dinv, n, st);
   }
   const double* Dv = jacobi ? dinv : nullptr;
@@ -989,6 +1144,7 @@ extern "C" int sf_cg_noalloc(sf_op* op, int mode, const double* b, double* x, do
                    std::to_string(kNoAllocMaxFree));
     SF_REQUIRE(mode == SF_CG_F64 || mode == SF_CG_F64_PLAIN, SF_ERR_UNSUPPORTED,
                "sf_cg_noalloc supports SF_CG_F64 and SF_CG_F64_PLAIN only");
+    SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_cg_noalloc does not take slab operators");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     double rel = 0.0;
     const int it = cg_f64_noalloc(op, mode == SF_CG_F64, b, x, reltol, maxiter, &rel, st);
