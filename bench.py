@@ -10,11 +10,12 @@ drawn from U[-1, 1] (seed 0) and is resident in HBM. Each timed step uses the
 next of 4 rotating x/y buffer pairs (1.09 GB in total, above the 126 MB L2),
 so a step never starts with its inputs in L2.
 
-With N > 1 (torchrun), every rank applies its own independent Q4 64^3
-problem: the apply of one problem has no exchange step in this
-configuration, so ranks are replicas (weak scaling). The timed region is
-bracketed by a barrier and a device synchronize, and the reported time is
-the maximum over ranks.
+With N > 1 (torchrun, one process per GPU), one problem of 64 x 64 x 64N
+cells is split into N z-slabs of 64^3 cells, one per rank (weak scaling:
+(256+1)^2 (256N+1) dofs in all). A step is one distributed apply: the halo
+exchange of the input (NCCL point-to-point, p + 1 planes per cut) and each
+rank's slab apply. The timed region is bracketed by a barrier and a device
+synchronize, and the reported time is the maximum over ranks.
 
 ``--impl reference`` times the reference's CPU path on this machine's host
 cores instead. Julia and Gridap are not available, so it runs the C
@@ -199,6 +200,99 @@ def time_tile_candidates(A, dev, reps=20):
     return out
 
 
+def run_slabs(args, sf, rank, world, dev):
+    """N > 1: one 64 x 64 x 64N problem, one z-slab of 64^3 cells per rank."""
+    import torch
+    import torch.distributed as dist
+    nz = NCELL * world
+    m = sf.SumFactorizationMap(3, (P,) * 3, (DEG,) * 3)
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, world), (NCELL, NCELL, nz))
+    D = sf.distributed.DistributedLazyMatrix(m, model, nparts=world, group=dist.group.WORLD,
+                                             device=dev)
+    D.autotune(torch.float64)
+    L = D.layouts[0]
+    n_total = (NCELL * P + 1) ** 2 * (nz * P + 1)
+    rng = np.random.default_rng(rank)
+    NBUF = 4
+    xs, ys = [], []
+    for _ in range(NBUF):
+        x = D.new_vector()
+        x[0][L.owned] = torch.from_numpy(rng.uniform(-1, 1, L.owned.stop - L.owned.start)).to(dev)
+        xs.append(x)
+        ys.append(D.new_vector())
+    for i in range(max(3, args.warmup)):
+        D.mul(ys[i % NBUF], xs[i % NBUF])
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        ev0.record()
+        for i in range(args.steps):
+            D.mul(ys[i % NBUF], xs[i % NBUF])
+        ev1.record()
+        torch.cuda.synchronize()
+    dist.barrier()
+    t = torch.tensor([ev0.elapsed_time(ev1)], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = t.item() / args.steps
+    value = n_total / (ms_step * 1e-3) / 1e9
+
+    # end to end: each rank's owned x from pinned host memory, the distributed apply,
+    # and its owned y back to pinned host memory, every step
+    e2e = None
+    if not args.no_e2e:
+        own = L.owned.stop - L.owned.start
+        xh = torch.empty(own, dtype=torch.float64).pin_memory()
+        yh = torch.empty(own, dtype=torch.float64).pin_memory()
+        xh.copy_(xs[0][0][L.owned].cpu())
+        ne2e = max(5, min(50, args.steps // 40))
+
+        def e2e_step():
+            xs[0][0][L.owned].copy_(xh, non_blocking=True)
+            D.mul(ys[0], xs[0])
+            yh.copy_(ys[0][0][L.owned], non_blocking=True)
+            torch.cuda.synchronize()
+        for _ in range(3):
+            e2e_step()
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne2e):
+            e2e_step()
+        te = torch.tensor([(time.perf_counter() - t0) / ne2e], device=dev)
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        te2e = te.item()
+        e2e = {"value": round(n_total / te2e / 1e9, 4), "unit": "GDOF/s",
+               "h2d_bytes_per_step": own * 8 * world, "d2h_bytes_per_step": own * 8 * world,
+               "ms_per_step": round(te2e * 1e3, 4),
+               "buffers": "pinned host, each rank's owned points, distributed apply"}
+    peaks = None
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    alg_bytes = n_total * 16 / world  # per rank (one launch)
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GDOF/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: owned x ~ U[-1,1] (rank r: seed r)",
+        "config": {"workload": f"Q4 64x64x{nz} affine hex (64^3 cells per rank), 5-pt Gauss, "
+                               "homogeneous Dirichlet, FP64 apply y=Ax",
+                   "n_cells": NCELL ** 3 * world, "order": P, "quad_points": 5,
+                   "n_dof_total": n_total, "kernel": "tiled-cartesian (z-slab)",
+                   "tile": {"f64": D.engines[0].kernel_name(torch.float64)},
+                   "l2": "4 rotating x/y buffer sets (> 126 MB L2 per rank)",
+                   "parallelism": f"z-slab x{world}, halo exchange over NCCL"},
+        "e2e": e2e,
+        "gpu_launches": args.steps,
+        "roofline": roofline_entry(alg_bytes / (ms_step * 1e-3) / 1e9, peaks, None),
+        "clocks": clk.summary(),
+    }
+    out["roofline"]["algorithmic_bytes_per_launch"] = alg_bytes
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -207,6 +301,10 @@ def run_ours(args, rank, world, local_rank):
     sf = g.load()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if world > 1:
+        out = run_slabs(args, sf, rank, world, dev)
+        dist.barrier()
+        return out
     if args.section is not None:
         fn = {"batched": run_batched, "adjoint": run_adjoint,
               "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,

@@ -236,6 +236,11 @@ class _SlabEngine:
         from .operator import _dtype_code
         check(lib.sf_autotune(self._h, _dtype_code(dtype), self._s()), self._h, "sf_autotune")
 
+    def kernel_name(self, dtype) -> str:
+        from .operator import _dtype_code
+        raw = lib.sf_kernel_name(self._h, _dtype_code(dtype))
+        return raw.decode() if raw else ""
+
     def cgd_start(self, b, x, r, p, q, s):
         check(lib.sf_cgd_start(self._h, *map(self._p, (b, x, r, p, q, s)), self._s()), self._h,
               "sf_cgd_start")
