@@ -69,6 +69,7 @@ struct CartParams {
   int nfx, nfy, nfz;  // free grid (inputs are read for z in [zlo, nfz))
   int zlo, nfz_out;   // lowest input z (-1 on a slab: the halo plane below); outputs z < nfz_out
   int ntx, nty, ntz;  // tiles
+  int tile0;          // first tile of the launch (CTA b applies tile tile0 + b)
   double* dot;  // non-null: dot[tile] = sum of x*y over the tile's outputs
 };
 
@@ -437,7 +438,7 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   EOMat<P, T> Mm, Km;
   Mm.load(Q.Me, Q.Mo);
   Km.load(Q.Ke, Q.Ko);
-  const int tile = blockIdx.x;
+  const int tile = Q.tile0 + (int)blockIdx.x;
   cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz, Q.zlo,
                                        Q.nfz_out,
                                        tile % Q.ntx, (tile / Q.ntx) % Q.nty,
@@ -611,8 +612,14 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   Q.nty = (plan.ny + EY - 1) / EY;
   Q.ntz = (plan.nz + EZ - 1) / EZ;
   Q.dot = fuse.dot;
-  const long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
+  long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
   SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
+  if (fuse.tz1 >= 0) {  // tile rows [tz0, tz1) only
+    SF_REQUIRE(fuse.tz0 >= 0 && fuse.tz0 < fuse.tz1 && fuse.tz1 <= Q.ntz, SF_ERR_ARG,
+               "tile-row range out of bounds");
+    Q.tile0 = fuse.tz0 * Q.ntx * Q.nty;
+    tiles = (long long)(fuse.tz1 - fuse.tz0) * Q.ntx * Q.nty;
+  }
   const size_t smem = (size_t)G::WORDS * sizeof(T);
   if (iso) {
     auto kern = k_cartesian<P, EX, EY, EZ, NT, true, T, MINB>;
@@ -807,6 +814,10 @@ void cartesian_diag(const CartesianPlan& plan, double* d, cudaStream_t stream) {
   const long long blocks = std::min<long long>((n + 255) / 256, 148LL * 16);
   k_cartesian_diag<<<(unsigned)blocks, 256, 0, stream>>>(Q);
   SF_CUDA_CHECK(cudaGetLastError());
+}
+
+int cartesian_tile_ez(const CartesianPlan& plan, int dtype) {
+  return pick(plan, dtype, plan.choice[dtype_slot(dtype)]).ez;
 }
 
 long long cartesian_tiles(const CartesianPlan& plan, int dtype) {

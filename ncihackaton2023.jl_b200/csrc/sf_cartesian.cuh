@@ -22,6 +22,7 @@ struct CartesianPlan {
 // Optional work fused into one apply of the CG loop.
 struct CartFuse {
   double* dot = nullptr;  // per-tile partial sums of x*y (cartesian_tiles entries)
+  int tz0 = 0, tz1 = -1;  // tz1 >= 0: apply only the tile rows tz0 <= tz < tz1 (z-rows of tiles)
 };
 
 // Builds the 1D operators; returns false when no tiled kernel exists for SB.
@@ -51,6 +52,8 @@ void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* 
                      cudaStream_t stream, const CartFuse& fuse = CartFuse{});
 // diag(A) at the points an apply writes (same layout as y; other points untouched).
 void cartesian_diag(const CartesianPlan& plan, double* d, cudaStream_t stream);
+// Cells per tile along z of the chosen candidate (a tile row covers EZ cell layers).
+int cartesian_tile_ez(const CartesianPlan& plan, int dtype);
 // Tiles (CTAs) of one apply with the chosen candidate: the entries CartFuse::dot receives.
 long long cartesian_tiles(const CartesianPlan& plan, int dtype);
 void cartesian_release(CartesianPlan& plan);

@@ -49,6 +49,9 @@ struct sf_op {
   size_t ws_bytes = 0;
   double* d_hx = nullptr;    // sf_mul_host staging
   double* d_hy = nullptr;
+  long long h_n = 0;         // their length
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};  // sf_mul_host: copy in, apply, copy out
+  std::vector<cudaEvent_t> pipe_ev;
   double* h_scalar = nullptr;  // pinned
   double* h_report = nullptr;  // mapped pinned: CG progress reports written by the device
   double* d_report = nullptr;  // its device address
@@ -199,6 +202,67 @@ long long owned_count(const sf_op* op) {
   const long long planes = (long long)(op->slab_z1 - op->slab_z0) * op->p -
                            (op->slab_z1 == op->mesh_nz ? 1 : 0);
   return planes * op->plane;
+}
+
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // pageable memory on older runtimes reports an error; clear it
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// sf_mul_host on the tiled Cartesian kernel with pinned host buffers: the z-levels
+// are copied in, applied and copied out in groups of tile rows on three streams,
+// so the two PCIe directions and the apply overlap. Group g can run once the levels
+// its tiles read (up to one cell above its last row) are on the device, and its
+// owned levels go back as soon as it is done. Returns false when it does not apply.
+bool mul_host_pipelined(sf_op* op, const double* x, double* y) {
+  if (!(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64)) || op->slab) return false;
+  if (!host_pinned(x) || !host_pinned(y)) return false;
+  const int P = op->p, nz = op->cells.nz;
+  const int ez = sf::cartesian_tile_ez(op->cart, SF_F64);
+  const int ntz = (nz + ez - 1) / ez;
+  const int groups = std::min(8, ntz);
+  if (groups < 2) return false;
+  const long long plane = op->plane, nfz = (long long)nz * P - 1;
+  for (cudaStream_t& q : op->pipe)
+    if (!q) SF_CUDA_CHECK(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+  while ((int)op->pipe_ev.size() < 2 * groups) {
+    cudaEvent_t e;
+    SF_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    op->pipe_ev.push_back(e);
+  }
+  cudaStream_t s_in = op->pipe[0], s_cmp = op->pipe[1], s_out = op->pipe[2];
+  long long copied = 0;  // planes [0, copied) of x are on their way to the device
+  for (int g = 0; g < groups; ++g) {
+    const int r0 = (int)((long long)ntz * g / groups), r1 = (int)((long long)ntz * (g + 1) / groups);
+    const long long need = std::min(nfz, (long long)(r1 * ez + 1) * P);  // input planes read
+    if (need > copied) {
+      SF_CUDA_CHECK(cudaMemcpyAsync(op->d_hx + copied * plane, x + copied * plane,
+                                    (size_t)((need - copied) * plane) * sizeof(double),
+                                    cudaMemcpyHostToDevice, s_in));
+      copied = need;
+    }
+    SF_CUDA_CHECK(cudaEventRecord(op->pipe_ev[2 * g], s_in));
+    SF_CUDA_CHECK(cudaStreamWaitEvent(s_cmp, op->pipe_ev[2 * g], 0));
+    sf::CartFuse rows;
+    rows.tz0 = r0;
+    rows.tz1 = r1;
+    sf::cartesian_apply(op->cart, SF_F64, op->d_hx, op->d_hy, s_cmp, rows);
+    SF_CUDA_CHECK(cudaEventRecord(op->pipe_ev[2 * g + 1], s_cmp));
+    SF_CUDA_CHECK(cudaStreamWaitEvent(s_out, op->pipe_ev[2 * g + 1], 0));
+    const long long o0 = (long long)r0 * ez * P, o1 = std::min(nfz, (long long)r1 * ez * P);
+    if (o1 > o0)
+      SF_CUDA_CHECK(cudaMemcpyAsync(y + o0 * plane, op->d_hy + o0 * plane,
+                                    (size_t)((o1 - o0) * plane) * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s_out));
+  }
+  SF_CUDA_CHECK(cudaStreamSynchronize(s_out));
+  SF_CUDA_CHECK(cudaStreamSynchronize(s_cmp));
+  SF_CUDA_CHECK(cudaStreamSynchronize(s_in));
+  return true;
 }
 
 // 1 / diag(A) on the owned points (zero elsewhere), cached.
@@ -512,6 +576,9 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_hy);
   if (op->h_scalar) cudaFreeHost(op->h_scalar);
   if (op->h_report) cudaFreeHost(op->h_report);
+  for (cudaStream_t q : op->pipe)
+    if (q) cudaStreamDestroy(q);
+  for (cudaEvent_t e : op->pipe_ev) cudaEventDestroy(e);
   sf::cartesian_release(op->cart);
   delete op;
   return SF_OK;
@@ -773,10 +840,16 @@ int sf_mul_host(sf_op* op, const double* x, double* y) {
     require_ready(op);
     SF_REQUIRE(x && y, SF_ERR_ARG, "null x or y");
     const size_t bytes = op->n_free * sizeof(double);
-    if (!op->d_hx) {
+    if (op->h_n != op->n_free) {
+      dfree(op->d_hx);
+      dfree(op->d_hy);
+      op->d_hx = op->d_hy = nullptr;
+      op->h_n = 0;
       op->d_hx = dalloc<double>(op->n_free);
       op->d_hy = dalloc<double>(op->n_free);
+      op->h_n = op->n_free;
     }
+    if (mul_host_pipelined(op, x, y)) return;
     cudaStream_t st = 0;
     SF_CUDA_CHECK(cudaMemcpyAsync(op->d_hx, x, bytes, cudaMemcpyHostToDevice, st));
     apply_impl(op, SF_F64, op->d_hx, op->d_hy, st);

@@ -128,6 +128,22 @@ def test_host_buffers_mul(sf):
     assert relerr(y2, y) < 1e-14
 
 
+@pytest.mark.parametrize("p,n", [(4, (5, 6, 11)), (2, (4, 3, 16)), (4, (3, 3, 7))])
+def test_pinned_host_mul_is_pipelined_and_exact(sf, p, n):
+    """With pinned host buffers sf_mul_host copies in, applies and copies out in
+    groups of tile rows on three streams; the result equals the device apply."""
+    torch = _torch()
+    A, V = build(sf, p, 2 * p, n)
+    assert A.uses_tiled_kernel()
+    x = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, A.n))
+    xh = x.clone().pin_memory()
+    yh = torch.full_like(x, float("nan")).pin_memory()
+    for _ in range(2):  # the second call reuses the streams and events
+        sf.mul(yh.numpy(), A, xh.numpy())
+        y_dev = A @ x.cuda()
+        assert torch.equal(yh, y_dev.cpu())
+
+
 def test_evaluate_cells_matches_map(sf):
     """The Map protocol: evaluate!(m, x_e, wq, jq, djq) for a batch of cells."""
     torch = _torch()
