@@ -463,16 +463,29 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
 
 def run_cg(sf, m, model, V, A, dev, maxiter=CG_MAXITER):
     """CG to relres 1e-10: the manufactured problem of the benchmark
-    (f = 3 pi^2 sin sin sin), and a rough right-hand side (b ~ U[-1,1], seed
-    1), both FP64 Jacobi CG and mixed precision (FP32 recurrence and apply,
-    FP64 reliable updates)."""
+    (f = 3 pi^2 sin sin sin; its right-hand side formed on the device by sf_rhs,
+    and on the host by numpy as a cross-check), and a rough right-hand side
+    (b ~ U[-1,1], seed 1), both FP64 Jacobi CG and mixed precision (FP32
+    recurrence and apply, FP64 reliable updates)."""
     import torch
-    b = torch.from_numpy(sf.assemble_rhs(m, V, lambda X: 3 * np.pi ** 2 * np.prod(np.sin(np.pi * X),
-                                                                               axis=-1))).to(dev)
+
+    def f(X):  # f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z) at (..., 3) device coordinates
+        return 3 * np.pi ** 2 * torch.prod(torch.sin(np.pi * X), dim=-1)
+    fq = f(sf.quadrature_points(A, dev))
+    b = sf.rhs(A, fq)  # matrix-free right-hand side on the device
+    torch.cuda.synchronize()
+    rhs_ms = _events_ms(lambda: sf.rhs(A, fq), 5)
+    t0 = time.perf_counter()
+    b_host = sf.assemble_rhs(m, V, lambda X: 3 * np.pi ** 2 * np.prod(np.sin(np.pi * X), axis=-1))
+    host_s = time.perf_counter() - t0
+    rhs_info = {"device_ms": round(rhs_ms, 3), "host_numpy_s": round(host_s, 2),
+                "max_rel_diff_device_vs_host": float(np.abs(b.cpu().numpy() - b_host).max() /
+                                                     np.abs(b_host).max())}
     X = V.free_dof_coordinates()
     u_exact = torch.from_numpy(np.prod(np.sin(np.pi * X), axis=1)).to(dev)
     res = _timed_solves(sf, A, b, u_exact, maxiter=maxiter)
     res["preconditioner"] = "Jacobi (matrix-free diagonal)"
+    res["rhs"] = rhs_info
     b_rough = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, V.num_free_dofs)).to(dev)
     res["rough_rhs"] = _timed_solves(sf, A, b_rough, maxiter=maxiter)
     return res

@@ -173,6 +173,17 @@ int sf_mul_host(sf_op* op, const double* x, double* y);
 int sf_evaluate_cells(sf_op* op, int dtype, int64_t ncells, const void* x_cells,
                       void* y_cells, void* stream);
 
+/*
+ * Right-hand side of the linear form v -> integral of f v over the mesh
+ * (the l(v) of profiling/drivers.jl:20, assembled by Gridap there), matrix-free:
+ * b = sum over cells of P_e^T (A0^T (x) A0^T (x) A0^T) (wq |djq| f), the scalar
+ * interpolation of src/SumFactorizationKernels.jl:15-38 transposed. fq: f at
+ * the quadrature points, [cell][SQ^D] FP64 device array, points in the order of
+ * the cell quantities (i1 fastest). b: n_free FP64 device array (overwritten;
+ * Dirichlet dofs get nothing, i.e. homogeneous Dirichlet data).
+ */
+int sf_rhs(sf_op* op, const double* fq, double* b, void* stream);
+
 /* diag(A) over the free dofs (device pointer of dtype), for Jacobi. */
 int sf_diagonal(sf_op* op, int dtype, void* d, void* stream);
 

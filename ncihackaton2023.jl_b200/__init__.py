@@ -13,10 +13,11 @@ from .fem import (CartesianDiscreteModel, FESpace, Measure, Table, TrialFESpace,
                   cell_quantities)
 from . import adjoint, batch, distributed
 from .operator import (LazyMatrix, SumFactorizationMap, assemble_rhs, cg, get_dimensional_parameters,
-                       mul, mul_multi)
+                       mul, mul_multi, quadrature_points, rhs)
 
 __all__ = [
     "CartesianDiscreteModel", "FESpace", "TrialFESpace", "Measure", "Table", "cell_quantities",
     "SumFactorizationMap", "get_dimensional_parameters", "LazyMatrix", "mul", "mul_multi", "cg",
-    "assemble_rhs", "SumFacError", "LIB_PATH", "fem", "adjoint", "batch", "distributed",
+    "assemble_rhs", "rhs", "quadrature_points", "SumFacError", "LIB_PATH", "fem", "adjoint",
+    "batch", "distributed",
 ]

@@ -60,6 +60,8 @@ struct GenParams {
   const double* gtab;
   long long gstride;
   const double* kappa;
+  const double* wdet;
+  long long wdet_stride;
 };
 
 template <int SB, int SQ>
@@ -401,6 +403,75 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   }
 }
 
+// Right-hand side of the linear form v -> integral of f v (profiling/drivers.jl:20):
+// b_e = (A^T (x) A^T (x) A^T) (w |det J| f) per cell, the scalar interpolation of
+// src/SumFactorizationKernels.jl:15-38 transposed, then assembled with atomics.
+// P.x holds f at the points ([cell][SQ^3]); one slot of SM^3 words per element,
+// the same in-place line passes as k_general.
+template <int SB, int SQ, bool EO>
+__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS, Shape<SB, SQ>::MINB)
+k_rhs(const __grid_constant__ GenParams<SB, SQ, double> P) {
+  using S = Shape<SB, SQ>;
+  using T = double;
+  constexpr int SM = S::SM, NQ = SQ * SQ * SQ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int el = threadIdx.x / S::NL;
+  const int l = threadIdx.x % S::NL;
+  const long long cell = (long long)blockIdx.x * S::EPB + el;
+  const bool valid = cell < P.ncells;
+  T* U = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SM3;
+  __shared__ T sMat[(!EO && kStageMats<T, SB, SQ>) ? 2 * SQ * SB : 1];
+  __shared__ __align__(16) T sEO[EO ? EOTables<SB, SQ>::TOTAL : 2];
+  if constexpr (EO) stage_eo<SB, SQ, T>(P, sEO);
+  else stage_mats<SB, SQ, T>(P, sMat);
+  auto at = [](int c3, int c2, int c1) { return (c3 * SM + c2) * SM + c1; };
+  auto load = [](const T* io, int stride, auto& u) {
+    asm volatile("" ::: "memory");
+    constexpr int N = sizeof(u) / sizeof(T);
+#pragma unroll
+    for (int c = 0; c < N; ++c) u[c] = io[c * stride];
+  };
+  // weighted point values
+  const double* wd = P.wdet + (valid ? cell : 0) * P.wdet_stride;
+  for (int q = l; q < NQ; q += S::NL) {
+    const int qi = q % SQ, qj = (q / SQ) % SQ, qk = q / (SQ * SQ);
+    U[at(qk, qj, qi)] = valid ? P.x[cell * NQ + q] * wd[q] : 0.0;
+  }
+  __syncthreads();
+  if (l < SQ * SQ) {  // z: lines (qi, qj)
+    const int qi = l % SQ, qj = l / SQ;
+    T* z = U + at(0, qj, qi);
+    T u[SQ];
+    load(z, SM * SM, u);
+    contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { z[r * SM * SM] = v; });
+  }
+  __syncthreads();
+  if (l < SQ * SB) {  // y: lines (qi, k)
+    const int qi = l % SQ, k = l / SQ;
+    T* yl = U + at(k, 0, qi);
+    T u[SQ];
+    load(yl, SM, u);
+    contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { yl[r * SM] = v; });
+  }
+  __syncthreads();
+  if (l < SB * SB) {  // x: lines (j, k)
+    const int j = l % SB, k = l / SB;
+    T* xl = U + at(k, j, 0);
+    T u[SQ];
+    load(xl, 1, u);
+    contract<2, EO, SB, SQ, T, SB, SQ>(sMat, sEO, P, u, [&](int r, T v) { xl[r] = v; });
+  }
+  __syncthreads();
+  if (!valid) return;
+  const CellOrigin org =
+      P.ids ? CellOrigin{0, 0, 0, 0, 0, 0} : cell_origin(cell, SB - 1, P.nx, P.ny, P.nz);
+  for (int pos = l; pos < S::S0; pos += S::NL) {
+    const int i = pos % SB, j = (pos / SB) % SB, k = pos / (SB * SB);
+    const long long id = P.ids ? (long long)P.ids[cell * S::S0 + pos] : cell_dof(org, i, j, k);
+    if (id >= 0) atomicAdd(P.y + id, U[at(k, j, i)]);
+  }
+}
+
 // Diagonal of the assembled operator: for each cell and tensor position a,
 // diag_e[a] = sum_q sum_{r,s} G_rs(q) dphi_a/dxi_r(q) dphi_a/dxi_s(q), with the
 // 3D basis gradient a product of 1D values. One thread per (cell, a); the sum
@@ -650,6 +721,8 @@ GenParams<SB, SQ, T> make_params(const double* A, const double* B, const Geometr
   P.gtab = geom.table;
   P.gstride = geom.table_stride;
   P.kappa = geom.kappa;
+  P.wdet = geom.wdet;
+  P.wdet_stride = geom.wdet_stride;
   return P;
 }
 
@@ -685,6 +758,44 @@ void run_general(int mode, const double* A, const double* B, const Cells& cells,
   SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
   SF_CUDA_CHECK(cudaGetLastError());
+}
+
+template <int SB, int SQ>
+void run_rhs(const double* A, const double* B, const Cells& cells, const Geometry& geom,
+             const double* fq, double* b, cudaStream_t stream) {
+  using S = Shape<SB, SQ>;
+  auto P = make_params<SB, SQ, double>(A, B, geom);
+  P.x = fq;
+  P.y = b;
+  P.ids = cells.ids;
+  P.ncells = cells.ncells;
+  P.nx = cells.nx;
+  P.ny = cells.ny;
+  P.nz = cells.nz;
+  if (cells.ncells == 0) return;
+  SF_REQUIRE(geom.wdet, SF_ERR_STATE, "no point weights: call sf_set_cell_quantities first");
+  const size_t smem = (size_t)S::EPB * S::SM3 * sizeof(double);
+  const long long blocks = (cells.ncells + S::EPB - 1) / S::EPB;
+  SF_REQUIRE(blocks < (1LL << 31), SF_ERR_ARG, "too many cells for one launch");
+  auto kern = centro_symmetric(A, B, SB, SQ) ? k_rhs<SB, SQ, true> : k_rhs<SB, SQ, false>;
+  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+using RhsFn = void (*)(const double*, const double*, const Cells&, const Geometry&, const double*,
+                       double*, cudaStream_t);
+
+RhsFn select_rhs(int SB, int SQ) {
+#define SF_CASE(sb, sq) \
+  if (SB == sb && SQ == sq) return &run_rhs<sb, sq>;
+#define SF_ROW(sb) SF_CASE(sb, sb - 1) SF_CASE(sb, sb) SF_CASE(sb, sb + 1) SF_CASE(sb, sb + 2)
+  SF_ROW(2) SF_ROW(3) SF_ROW(4) SF_ROW(5) SF_ROW(6) SF_ROW(7) SF_ROW(8)
+  SF_CASE(9, 8) SF_CASE(9, 9) SF_CASE(9, 10)
+  SF_CASE(10, 9) SF_CASE(10, 10)
+#undef SF_ROW
+#undef SF_CASE
+  return nullptr;
 }
 
 using RunFn = void (*)(int, const double*, const double*, const Cells&, long long, const int32_t*,
@@ -775,6 +886,15 @@ void launch_general_apply(int dtype, int SB, int SQ, const double* A, const doub
 void launch_general_diag(int dtype, int SB, int SQ, const double* A, const double* B,
                          const Cells& cells, const Geometry& geom, void* d, cudaStream_t stream) {
   select_dtype(dtype, SB, SQ)(2, A, B, cells, cells.ncells, nullptr, geom, nullptr, d, stream);
+}
+
+void launch_general_rhs(int SB, int SQ, const double* A, const double* B, const Cells& cells,
+                        const Geometry& geom, const double* fq, double* b, cudaStream_t stream) {
+  RhsFn f = select_rhs(SB, SQ);
+  if (!f)
+    throw Error(SF_ERR_UNSUPPORTED, "no right-hand-side kernel for SB=" + std::to_string(SB) +
+                                        " SQ=" + std::to_string(SQ));
+  f(A, B, cells, geom, fq, b, stream);
 }
 
 void launch_general_evaluate(int dtype, int SB, int SQ, const double* A, const double* B,

@@ -44,6 +44,8 @@ struct Geometry {
   const double* table = nullptr;  // table: [cell][6][SQ^3]
   long long table_stride = 0;     // doubles per cell (0 = one cell shared by all)
   const double* kappa = nullptr;  // [cell][SQ^3] or null
+  const double* wdet = nullptr;   // w_q |det J| at the points, [cell][SQ^3] (the right-hand side)
+  long long wdet_stride = 0;      // doubles per cell (0 = one cell shared by all)
 };
 
 // Gather/scatter description shared by the element kernels.
@@ -57,6 +59,10 @@ struct Cells {
 
 // Launchers implemented in kernels_general.cu. A, B: SQ x SB row-major
 // ([qp][basis]) in the kernel's 1D order.
+// b += sum over cells of P_e^T (A^T (x) A^T (x) A^T) (w |det J| f) with f at the points,
+// fq [cell][SQ^3] (FP64; b must be zeroed first).
+void launch_general_rhs(int SB, int SQ, const double* A, const double* B, const Cells& cells,
+                        const Geometry& geom, const double* fq, double* b, cudaStream_t stream);
 void launch_general_apply(int dtype, int SB, int SQ, const double* A, const double* B,
                           const Cells& cells, const Geometry& geom, const void* x, void* y,
                           cudaStream_t stream);

@@ -34,6 +34,7 @@ struct sf_op {
   int32_t* d_t2l = nullptr;
   sf::Geometry geom;
   double* d_gtab = nullptr;
+  double* d_wdet = nullptr;  // w |det J| at the points (right-hand side)
   double* d_kappa = nullptr;
   long long cq_cells = -1;  // -1 = unset, 0 = fill (one cell for all)
   bool cartesian_ok = false;
@@ -568,6 +569,7 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_ids);
   dfree(op->d_t2l);
   dfree(op->d_gtab);
+  dfree(op->d_wdet);
   dfree(op->d_kappa);
   dfree(op->d_diag);
   dfree(op->d_dinv);
@@ -700,11 +702,13 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
     // G = wq*djq*jq^T jq at every point (src/SumFactorizationKernels.jl:174-216)
     std::vector<double> G((size_t)nc * 6 * nq);
     std::vector<double> H((size_t)nc * 6 * nq);  // djq*jq^T jq (without the weight)
+    std::vector<double> WD((size_t)nc * nq);     // wq*djq (the right-hand side's weights)
     static const int rr[6] = {0, 1, 2, 0, 0, 1}, kk[6] = {0, 1, 2, 1, 2, 2};
     for (long long c = 0; c < nc; ++c)
       for (int q = 0; q < nq; ++q) {
         const double* J = jq + ((size_t)c * nq + q) * D * D;
         const double w = wq[(size_t)c * nq + q], dj = djq[(size_t)c * nq + q];
+        WD[(size_t)c * nq + q] = w * dj;
         for (int m = 0; m < 6; ++m) {
           double acc = 0.0;
           for (int l = 0; l < D; ++l) acc += J[l + D * rr[m]] * J[l + D * kk[m]];
@@ -765,6 +769,21 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
       g.table = op->d_gtab;
       g.table_stride = same ? 0 : 6LL * nq;
     }
+    bool wsame = true;
+    for (long long c = 1; c < nc && wsame; ++c)
+      for (int q = 0; q < nq; ++q)
+        if (WD[(size_t)c * nq + q] != WD[q]) {
+          wsame = false;
+          break;
+        }
+    dfree(op->d_wdet);
+    op->d_wdet = nullptr;
+    const long long nw = wsame ? 1 : nc;
+    op->d_wdet = dalloc<double>((size_t)nw * nq);
+    SF_CUDA_CHECK(cudaMemcpy(op->d_wdet, WD.data(), (size_t)nw * nq * sizeof(double),
+                             cudaMemcpyHostToDevice));
+    g.wdet = op->d_wdet;
+    g.wdet_stride = wsame ? 0 : nq;
     op->geom = g;
     op->cq_cells = (fill || same) ? 0 : nc;
     invalidate_caches(op);
@@ -873,6 +892,19 @@ int sf_evaluate_cells(sf_op* op, int dtype, int64_t ncells, const void* x_cells,
     sf::launch_general_evaluate(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), ncells,
                                 op->d_t2l, op->geom, x_cells, y_cells,
                                 static_cast<cudaStream_t>(stream));
+  });
+}
+
+int sf_rhs(sf_op* op, const double* fq, double* b, void* stream) {
+  if (!op) return SF_ERR_ARG;
+  return guarded(op, [&] {
+    require_ready(op);
+    SF_REQUIRE(fq && b, SF_ERR_ARG, "null fq or b");
+    SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_rhs does not take slab operators");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SF_CUDA_CHECK(cudaMemsetAsync(b, 0, op->n_free * sizeof(double), st));
+    sf::launch_general_rhs(op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, fq, b,
+                           st);
   });
 }
 

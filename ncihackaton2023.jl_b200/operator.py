@@ -326,6 +326,38 @@ def cg(A: LazyMatrix, b, x=None, reltol: float = 1e-10, maxiter: int | None = No
     return x, info
 
 
+def quadrature_points(A: LazyMatrix, device=None) -> "torch.Tensor":
+    """(ncells, SQ^3, 3) physical coordinates of every cell's quadrature points
+    (trilinear cell map, point index i1 fastest), computed on ``device``."""
+    device = device or torch.device("cuda")
+    q1 = torch.as_tensor(np.asarray(A.m.points), dtype=torch.float64)
+    qz, qy, qx = torch.meshgrid(q1, q1, q1, indexing="ij")
+    pts = torch.stack([qx.reshape(-1), qy.reshape(-1), qz.reshape(-1)], dim=1)
+    N = torch.ones(pts.shape[0], 8, dtype=torch.float64)
+    for v in range(8):
+        for a, bit in enumerate(((v & 1), (v >> 1) & 1, (v >> 2) & 1)):
+            N[:, v] *= pts[:, a] if bit else 1.0 - pts[:, a]
+    X = torch.as_tensor(A.model.vertices[A.model.cell_vertices()], dtype=torch.float64)
+    return torch.einsum("qv,cvj->cqj", N.to(device), X.to(device))
+
+
+def rhs(A: LazyMatrix, f) -> "torch.Tensor":
+    """b_i = integral of f phi_i (homogeneous Dirichlet data) on the device, by the
+    matrix-free kernel behind sf_rhs. ``f``: a (ncells, SQ^3) float64 CUDA tensor of
+    values at the quadrature points, or a function mapping a (..., 3) coordinate
+    tensor to values (evaluated at ``quadrature_points(A)``)."""
+    if callable(f):
+        f = f(quadrature_points(A))
+    fq = f.contiguous()
+    nq = A.m.SQ[0] ** 3
+    if fq.dtype != torch.float64 or not fq.is_cuda or fq.numel() != A.model.num_cells * nq:
+        raise ValueError("f at the points must be a float64 CUDA tensor of shape (ncells, SQ^3)")
+    b = torch.empty(A.n, dtype=torch.float64, device=fq.device)
+    check(lib.sf_rhs(A._h, C.c_void_p(fq.data_ptr()), C.c_void_p(b.data_ptr()), _stream()), A._h,
+          "sf_rhs")
+    return b
+
+
 def assemble_rhs(m: SumFactorizationMap, V: fem.FESpace, f, chunk: int = 32768) -> np.ndarray:
     """b_i = integral of f phi_i over the mesh with homogeneous Dirichlet data (the
     linear form ``v -> int(v*f)dOmega`` of profiling/drivers.jl:20), formed on
