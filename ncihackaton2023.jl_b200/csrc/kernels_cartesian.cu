@@ -428,6 +428,173 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   if (threadIdx.x == 0) *dot = t;
 }
 
+
+// ---------------------------------------------------------------------------
+// 2D (quadrilateral Q_p) tiled apply on an nx x ny Cartesian mesh:
+//   y = cx Kx(x)My + cy Mx(x)Ky  (K along the first factor's axis),
+// the 2D form of the Kronecker identity above (the domain of the reference's
+// own 2D GPU kernels, src/GPUKernels.jl). A CTA owns EX x EY cells and
+// recomputes a one-cell halo; nothing is scattered.
+//   pass 1: y-line segments of CY cells straight from global memory into
+//           registers: t1 = My x -> T1, t2 = Ky x -> T2 (owned rows, all columns);
+//   pass 2: x-line segments of CX cells: every thread first loads its t1, t2
+//           segment into registers, then (after a barrier) writes
+//           cx Kx t1 + cy Mx t2 over its own owned points of T1;
+//   store:  the owned box of T1 back to global memory, coalesced.
+// ---------------------------------------------------------------------------
+template <int P, typename T>
+struct CartParams2 {
+  T Me[EO<P>::UE], Mo[EO<P>::UO];
+  T Ke[EO<P>::UE], Ko[EO<P>::UO];
+  T cx, cy;
+  const T* x;
+  T* y;
+  int nfx, nfy;  // free grid
+  int ntx, nty;  // tiles
+};
+
+template <int P, int EX, int EY>
+struct Tile2 {
+  static constexpr int BX = (EX + 1) * P + 1, BY = (EY + 1) * P + 1;
+  static constexpr int OX = EX * P, OY = EY * P;
+  static constexpr int PX = BX | 1;  // odd pitch: threads on different rows hit different banks
+  static constexpr int TS = OY * PX;
+  static constexpr int WORDS = 2 * TS;
+};
+
+// One segment of E cells of a line in registers (c[0 .. E*P+P]): out(o, M c, K c) for the
+// segment's outputs o = 0 .. E*P-1 (line points 1 .. E*P).
+template <int P, int E, typename T, typename Out>
+__device__ __forceinline__ void seg_mk(const EOMat<P, T>& Mm, const EOMat<P, T>& Km,
+                                       const T (&c)[E * P + P + 1], const Out& out) {
+  T cm = T(0), ck = T(0);
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    T u[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; ++m) u[m] = c[k * P + m];
+    const Split<P, T> s = split<P, T>(u);
+    Acc<P, T> am, ak;
+    am.zero();
+    ak.zero();
+    mac<P, T>(Mm, s, am.e, am.o);
+    mac<P, T>(Km, s, ak.e, ak.o);
+    if (k > 0) out(k * P - 1, am.at(0) + cm, ak.at(0) + ck);
+#pragma unroll
+    for (int m = 1; m < P; ++m) out(k * P + m - 1, am.at(m), ak.at(m));
+    cm = am.at(P);
+    ck = ak.at(P);
+  }
+  T u[P + 1];
+#pragma unroll
+  for (int m = 0; m <= P; ++m) u[m] = c[E * P + m];
+  const Split<P, T> s = split<P, T>(u);
+  out(E * P - 1, mac_row0<P, T>(Mm, s, cm), mac_row0<P, T>(Km, s, ck));
+}
+
+// out(o, K a + M b) over a segment of E cells held in registers.
+template <int P, int E, typename T, typename Out>
+__device__ __forceinline__ void seg_kamb(const EOMat<P, T>& Km, const EOMat<P, T>& Mm,
+                                         const T (&a)[E * P + P + 1], const T (&b)[E * P + P + 1],
+                                         const Out& out) {
+  T carry = T(0);
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    T ua[P + 1], ub[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; ++m) {
+      ua[m] = a[k * P + m];
+      ub[m] = b[k * P + m];
+    }
+    const Split<P, T> sa = split<P, T>(ua), sb = split<P, T>(ub);
+    Acc<P, T> acc;
+    acc.zero();
+    mac<P, T>(Km, sa, acc.e, acc.o);
+    mac<P, T>(Mm, sb, acc.e, acc.o);
+    if (k > 0) out(k * P - 1, acc.at(0) + carry);
+#pragma unroll
+    for (int m = 1; m < P; ++m) out(k * P + m - 1, acc.at(m));
+    carry = acc.at(P);
+  }
+  T ua[P + 1], ub[P + 1];
+#pragma unroll
+  for (int m = 0; m <= P; ++m) {
+    ua[m] = a[E * P + m];
+    ub[m] = b[E * P + m];
+  }
+  const Split<P, T> sa = split<P, T>(ua), sb = split<P, T>(ub);
+  out(E * P - 1, mac_row0<P, T>(Mm, sb, mac_row0<P, T>(Km, sa, carry)));
+}
+
+template <int P, int EX, int EY, int CX, int CY, int NT, bool ISO, typename T, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+k_cartesian2d(const __grid_constant__ CartParams2<P, T> Q) {
+  using G = Tile2<P, EX, EY>;
+  constexpr int SY = EY / CY, NY = CY * P + P + 1;
+  constexpr int SX = EX / CX, NX = CX * P + P + 1;
+  static_assert(EY % CY == 0 && EX % CX == 0, "segments must divide the tile");
+  static_assert(G::OY * SX <= NT, "pass 2 holds one segment per thread");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* T1 = reinterpret_cast<T*>(smem_raw);
+  T* T2 = T1 + G::TS;
+  EOMat<P, T> Mm, Km;
+  Mm.load(Q.Me, Q.Mo);
+  Km.load(Q.Ke, Q.Ko);
+  const int tx = (int)blockIdx.x % Q.ntx, ty = (int)blockIdx.x / Q.ntx;
+  const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1;
+
+  // pass 1: y segments (column x, cells sy*CY ..), inputs from global memory
+  for (int w = threadIdx.x; w < G::BX * SY; w += NT) {
+    const int x = w % G::BX, sy = w / G::BX;
+    const int fx = fx0 + x, fyb = fy0 + sy * CY * P;
+    const bool inx = (unsigned)fx < (unsigned)Q.nfx;
+    T c[NY];
+#pragma unroll
+    for (int i = 0; i < NY; ++i) {
+      const int fy = fyb + i;
+      c[i] = (inx && (unsigned)fy < (unsigned)Q.nfy) ? __ldg(Q.x + fx + (long long)Q.nfx * fy)
+                                                     : T(0);
+    }
+    seg_mk<P, CY, T>(Mm, Km, c, [&](int o, T m, T k) {
+      const int yo = sy * CY * P + o;
+      T1[yo * G::PX + x] = m;
+      T2[yo * G::PX + x] = k;
+    });
+  }
+  __syncthreads();
+
+  // pass 2: x segments (row yo, cells sx*CX ..): load, barrier, write in place
+  const int w = threadIdx.x;
+  const bool active = w < G::OY * SX;
+  const int yo = w % G::OY, sx = w / G::OY;
+  T a[NX], b[NX];
+  if (active) {
+    const T* r1 = T1 + yo * G::PX + sx * CX * P;
+    const T* r2 = T2 + yo * G::PX + sx * CX * P;
+#pragma unroll
+    for (int i = 0; i < NX; ++i) {
+      a[i] = ISO ? r1[i] : r1[i] * Q.cx;
+      b[i] = ISO ? r2[i] : r2[i] * Q.cy;
+    }
+  }
+  __syncthreads();
+  if (active) {
+    T* o1 = T1 + yo * G::PX + sx * CX * P;
+    seg_kamb<P, CX, T>(Km, Mm, a, b, [&](int o, T v) { o1[o] = ISO ? v * Q.cx : v; });
+  }
+  __syncthreads();
+
+  // store the owned box (free coordinates start at e0 * p)
+  const int ox0 = fx0 + 1, oy0 = fy0 + 1;
+  const bool full = ox0 + G::OX <= Q.nfx && oy0 + G::OY <= Q.nfy;
+  T* ybase = Q.y + (long long)ox0 + (long long)Q.nfx * oy0;
+  for (int i = threadIdx.x; i < G::OX * G::OY; i += NT) {
+    const int xo = i % G::OX, yr = i / G::OX;
+    if (full || (ox0 + xo < Q.nfx && oy0 + yr < Q.nfy))
+      ybase[xo + (long long)Q.nfx * yr] = T1[yr * G::PX + xo];
+  }
+}
+
 template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
 k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
@@ -456,6 +623,7 @@ struct DiagParams {
   double c[3];
   double* d;  // first written point
   int p, nfx, nfy, nfz_out;
+  int D;      // 2: d = cx dK(x) dM(y) + cy dM(x) dK(y) over nfx x nfy points
 };
 
 __global__ void k_cartesian_diag(const __grid_constant__ DiagParams Q) {
@@ -470,9 +638,12 @@ __global__ void k_cartesian_diag(const __grid_constant__ DiagParams Q) {
       const int l = g % Q.p;
       return l == 0 ? D[0] + D[Q.p] : D[l];
     };
-    Q.d[i] = Q.c[0] * d1(Q.Kd, gx) * d1(Q.Md, gy) * d1(Q.Md, gz) +
-             Q.c[1] * d1(Q.Md, gx) * d1(Q.Kd, gy) * d1(Q.Md, gz) +
-             Q.c[2] * d1(Q.Md, gx) * d1(Q.Md, gy) * d1(Q.Kd, gz);
+    if (Q.D == 2)
+      Q.d[i] = Q.c[0] * d1(Q.Kd, gx) * d1(Q.Md, gy) + Q.c[1] * d1(Q.Md, gx) * d1(Q.Kd, gy);
+    else
+      Q.d[i] = Q.c[0] * d1(Q.Kd, gx) * d1(Q.Md, gy) * d1(Q.Md, gz) +
+               Q.c[1] * d1(Q.Md, gx) * d1(Q.Kd, gy) * d1(Q.Md, gz) +
+               Q.c[2] * d1(Q.Md, gx) * d1(Q.Md, gy) * d1(Q.Kd, gz);
   }
 }
 
@@ -633,6 +804,36 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
+// One launch of the 2D tile configuration (EX x EY cells, x/y segments of CX/CY cells).
+template <int P, typename T, int EX, int EY, int CX, int CY, int NT, int MINB>
+void run_tile2(const CartesianPlan& plan, const void* x, void* y, const CartFuse& fuse,
+               cudaStream_t st) {
+  using G = Tile2<P, EX, EY>;
+  SF_REQUIRE(!fuse.dot && fuse.tz1 < 0, SF_ERR_UNSUPPORTED,
+             "the 2D apply has no fused dot or tile-row range");
+  CartParams2<P, T> Q{};
+  fill_eo<P, T>(plan.M, 1.0, Q.Me, Q.Mo);
+  fill_eo<P, T>(plan.K, 1.0, Q.Ke, Q.Ko);
+  const double cx = plan.c[0], cy = plan.c[1];
+  const bool iso = cx == cy;
+  Q.cx = (T)cx;
+  Q.cy = (T)cy;
+  Q.x = static_cast<const T*>(x);
+  Q.y = static_cast<T*>(y);
+  Q.nfx = plan.nx * P - 1;
+  Q.nfy = plan.ny * P - 1;
+  Q.ntx = (plan.nx + EX - 1) / EX;
+  Q.nty = (plan.ny + EY - 1) / EY;
+  const long long tiles = (long long)Q.ntx * Q.nty;
+  SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
+  const size_t smem = (size_t)G::WORDS * sizeof(T);
+  auto kern = iso ? k_cartesian2d<P, EX, EY, CX, CY, NT, true, T, MINB>
+                  : k_cartesian2d<P, EX, EY, CX, CY, NT, false, T, MINB>;
+  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
 using RunFn = void (*)(const CartesianPlan&, const void*, void*, const CartFuse&, cudaStream_t);
 using BatchFn = void (*)(const CartesianPlan&, const void*, int, long long, unsigned long long*,
                          bool, cudaStream_t);
@@ -682,11 +883,57 @@ template <> struct Cands<7, float> { static constexpr Candidate c[] = {SF_TILE(7
 template <> struct Cands<8, float> { static constexpr Candidate c[] = {SF_TILE(8, float, 2, 2, 1, 256, 2)}; };
 #undef SF_TILE
 
+// 2D candidates: tiles of about 64 x 64 points; pass 2 gives every thread one x segment.
+#define SF_TILE2(P_, T_, EX_, EY_, CX_, CY_, NT_, MINB_)                                  \
+  {&run_tile2<P_, T_, EX_, EY_, CX_, CY_, NT_, MINB_>, nullptr, EX_, EY_, 0,             \
+   #EX_ "x" #EY_ " cells, segments " #CX_ "/" #CY_ ", " #NT_ " thr, " #MINB_ "/SM"}
+template <int P, typename T>
+struct Cands2;
+#define SF_C2(P_, ...)                                                                     \
+  template <> struct Cands2<P_, double> { static constexpr Candidate c[] = {__VA_ARGS__}; };
+#define SF_T2D(P_, EX_, EY_, CX_, CY_, NT_, MINB_) SF_TILE2(P_, double, EX_, EY_, CX_, CY_, NT_, MINB_)
+#define SF_T2F(P_, EX_, EY_, CX_, CY_, NT_, MINB_) SF_TILE2(P_, float, EX_, EY_, CX_, CY_, NT_, MINB_)
+SF_C2(1, SF_T2D(1, 64, 64, 16, 16, 256, 2))
+SF_C2(2, SF_T2D(2, 32, 32, 8, 8, 256, 2))
+SF_C2(3, SF_T2D(3, 20, 20, 5, 5, 256, 2))
+SF_C2(4, SF_T2D(4, 16, 16, 4, 4, 256, 2), SF_T2D(4, 16, 16, 2, 4, 512, 1))
+SF_C2(5, SF_T2D(5, 12, 12, 3, 3, 256, 2))
+SF_C2(6, SF_T2D(6, 10, 8, 2, 2, 256, 2))
+SF_C2(7, SF_T2D(7, 8, 8, 2, 2, 256, 2))
+SF_C2(8, SF_T2D(8, 8, 8, 2, 2, 256, 2))
+#undef SF_C2
+#define SF_C2(P_, ...)                                                                     \
+  template <> struct Cands2<P_, float> { static constexpr Candidate c[] = {__VA_ARGS__}; };
+SF_C2(1, SF_T2F(1, 64, 64, 16, 16, 256, 2))
+SF_C2(2, SF_T2F(2, 32, 32, 8, 8, 256, 2))
+SF_C2(3, SF_T2F(3, 20, 20, 5, 5, 256, 2))
+SF_C2(4, SF_T2F(4, 16, 16, 4, 4, 256, 2), SF_T2F(4, 16, 16, 2, 4, 512, 1))
+SF_C2(5, SF_T2F(5, 12, 12, 3, 3, 256, 2))
+SF_C2(6, SF_T2F(6, 10, 8, 2, 2, 256, 2))
+SF_C2(7, SF_T2F(7, 8, 8, 2, 2, 256, 2))
+SF_C2(8, SF_T2F(8, 8, 8, 2, 2, 256, 2))
+#undef SF_C2
+#undef SF_T2D
+#undef SF_T2F
+#undef SF_TILE2
+
 template <typename T, int P>
 int cand_count() { return (int)(sizeof(Cands<P, T>::c) / sizeof(Candidate)); }
 
+template <typename T, int P>
+int cand2_count() { return (int)(sizeof(Cands2<P, T>::c) / sizeof(Candidate)); }
+
 template <typename T>
-const Candidate& candidate(int SB, int k) {
+const Candidate& candidate(int D, int SB, int k) {
+  if (D == 2) {
+    switch (SB - 1) {
+#define SF_CASE(P_) \
+  case P_: return Cands2<P_, T>::c[k < cand2_count<T, P_>() ? k : 0];
+      SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+      default: throw Error(SF_ERR_UNSUPPORTED, "no 2D tiled Cartesian kernel for this order");
+    }
+  }
   switch (SB - 1) {
 #define SF_CASE(P_) \
   case P_: return Cands<P_, T>::c[k < cand_count<T, P_>() ? k : 0];
@@ -697,31 +944,33 @@ const Candidate& candidate(int SB, int k) {
 }
 
 template <typename T>
-int candidates_for(int SB) {
+int candidates_for(int D, int SB) {
   switch (SB - 1) {
 #define SF_CASE(P_) \
-  case P_: return cand_count<T, P_>();
+  case P_: return D == 2 ? cand2_count<T, P_>() : cand_count<T, P_>();
     SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
 #undef SF_CASE
     default: return 0;
   }
 }
 
-int candidate_count(int SB, int dtype) {
-  return dtype == SF_F64 ? candidates_for<double>(SB) : candidates_for<float>(SB);
+int candidate_count(int D, int SB, int dtype) {
+  return dtype == SF_F64 ? candidates_for<double>(D, SB) : candidates_for<float>(D, SB);
 }
 
 const Candidate& pick(const CartesianPlan& plan, int dtype, int k) {
-  return dtype == SF_F64 ? candidate<double>(plan.SB, k) : candidate<float>(plan.SB, k);
+  return dtype == SF_F64 ? candidate<double>(plan.D, plan.SB, k)
+                         : candidate<float>(plan.D, plan.SB, k);
 }
 
 }  // namespace
 
 bool cartesian_prepare(CartesianPlan& plan, int SB, int SQ, const double* A, const double* B,
-                       const double* w1, const double* G0, int nx, int ny, int nz) {
+                       const double* w1, const double* G0, int nx, int ny, int nz, int D) {
   plan.ready = false;
   if (SB < 2 || SB > 9) return false;
-  if (!(G0[0] > 0 && G0[1] > 0 && G0[2] > 0)) return false;
+  if (!(G0[0] > 0 && G0[1] > 0 && (D == 2 || G0[2] > 0))) return false;
+  plan.D = D;
   plan.SB = SB;
   plan.SQ = SQ;
   plan.nx = nx;
@@ -774,7 +1023,7 @@ static int dtype_slot(int dtype) {
 
 int cartesian_candidates(const CartesianPlan& plan, int dtype) {
   dtype_slot(dtype);
-  return candidate_count(plan.SB, dtype);
+  return candidate_count(plan.D, plan.SB, dtype);
 }
 
 const char* cartesian_candidate_name(const CartesianPlan& plan, int dtype, int k) {
@@ -808,6 +1057,8 @@ void cartesian_diag(const CartesianPlan& plan, double* d, cudaStream_t stream) {
   Q.nfx = plan.nx * P - 1;
   Q.nfy = plan.ny * P - 1;
   Q.nfz_out = plan.slab ? plan.nz * P - (plan.slab_top ? 1 : 0) : plan.nz * P - 1;
+  Q.D = plan.D;
+  if (plan.D == 2) Q.nfz_out = 1;
   Q.d = d + (plan.slab ? (long long)Q.nfx * Q.nfy : 0);
   const long long n = (long long)Q.nfx * Q.nfy * Q.nfz_out;
   if (n <= 0) return;

@@ -17,6 +17,7 @@ struct CartesianPlan {
   // (one halo plane below, p above); outputs on levels z0 p + 1 .. (z0 + nz) p, the last one
   // left out when it is the mesh's Dirichlet boundary (slab_top)
   bool slab = false, slab_top = false;
+  int D = 3;  // 2: an nx x ny quadrilateral mesh (nz unused)
 };
 
 // Optional work fused into one apply of the CG loop.
@@ -27,7 +28,7 @@ struct CartFuse {
 
 // Builds the 1D operators; returns false when no tiled kernel exists for SB.
 bool cartesian_prepare(CartesianPlan& plan, int SB, int SQ, const double* A, const double* B,
-                       const double* w1, const double* G0, int nx, int ny, int nz);
+                       const double* w1, const double* G0, int nx, int ny, int nz, int D = 3);
 bool cartesian_supported(const CartesianPlan& plan, int dtype);
 // Tile-shape candidates for the plan's order and dtype (timed by sf_autotune).
 int cartesian_candidates(const CartesianPlan& plan, int dtype);

@@ -120,7 +120,8 @@ void rebuild_kernel_basis(sf_op* op) {
       op->A[q * SB + op->perm[j]] = op->A_user[q * SB + j];
       op->B[q * SB + op->perm[j]] = op->B_user[q * SB + j];
     }
-  const int nloc = SB * SB * SB;
+  int nloc = 1;
+  for (int d = 0; d < op->D; ++d) nloc *= SB;
   std::vector<int32_t> t2l(nloc, -1);
   for (int k = 0; k < nloc; ++k) t2l[tensor_pos(op, k)] = k;
   for (int v : t2l)
@@ -153,7 +154,7 @@ void update_cartesian(sf_op* op) {
     return;
   op->cartesian_ok = sf::cartesian_prepare(op->cart, op->SB, op->SQ, op->A.data(), op->B.data(),
                                            op->geom.w1, G, op->cells.nx, op->cells.ny,
-                                           op->cells.nz);
+                                           op->cells.nz, op->D);
   op->cart.slab = op->slab;
   op->cart.slab_top = op->slab && op->slab_z1 == op->mesh_nz;
 }
@@ -171,6 +172,9 @@ void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
   SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED,
              "a slab operator needs the tiled Cartesian kernel (axis-aligned affine cells, "
              "constant coefficient)");
+  SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED,
+             "D = 2 runs on the tiled Cartesian kernel only (axis-aligned affine cells, "
+             "constant coefficient)");
   SF_CUDA_CHECK(cudaMemsetAsync(y, 0, op->n_free * es, st));
   sf::launch_general_apply(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
                            x, y, st);
@@ -185,6 +189,7 @@ void compute_diag(sf_op* op, double* d, cudaStream_t st) {
     return;
   }
   SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "a slab operator needs the tiled Cartesian kernel");
+  SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "D = 2 runs on the tiled Cartesian kernel only");
   sf::launch_general_diag(SF_F64, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
                           d, st);
 }
@@ -220,7 +225,8 @@ bool host_pinned(const void* p) {
 // its tiles read (up to one cell above its last row) are on the device, and its
 // owned levels go back as soon as it is done. Returns false when it does not apply.
 bool mul_host_pipelined(sf_op* op, const double* x, double* y) {
-  if (!(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64)) || op->slab) return false;
+  if (!(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64)) || op->slab || op->D != 3)
+    return false;
   if (!host_pinned(x) || !host_pinned(y)) return false;
   const int P = op->p, nz = op->cells.nz;
   const int ez = sf::cartesian_tile_ez(op->cart, SF_F64);
@@ -355,8 +361,9 @@ const double* read_state(sf_op* op, const double* s, cudaStream_t st) {
 constexpr int kRR = 0, kBB = sf::CG_BB - sf::CG_RR, kDone = sf::CG_DONE - sf::CG_RR,
               kIters = sf::CG_ITERS - sf::CG_RR;
 
+// The 3D tiled kernel, whose store phase can also form the CG's (p, Ap) partial sums.
 bool tiled(const sf_op* op, int dtype) {
-  return op->cartesian_ok && sf::cartesian_supported(op->cart, dtype);
+  return op->cartesian_ok && op->D == 3 && sf::cartesian_supported(op->cart, dtype);
 }
 
 // Partial-sum entries the CG reductions of this operator need.
@@ -526,8 +533,8 @@ int sf_create(sf_op** out, int D, int SB, int SQ, const double* A0, const double
               const int32_t* dof_map) {
   if (!out) return SF_ERR_ARG;
   *out = nullptr;
-  if (D == 2) return SF_ERR_UNSUPPORTED;
-  if (D != 3 || SB < 2 || SB > sf::kMaxSB || SQ < 1 || SQ > sf::kMaxSQ || !A0 || !B0 || !dof_map)
+  if (D != 2 && D != 3) return SF_ERR_UNSUPPORTED;
+  if (SB < 2 || SB > sf::kMaxSB || SQ < 1 || SQ > sf::kMaxSQ || !A0 || !B0 || !dof_map)
     return SF_ERR_ARG;
   sf_op* op = new (std::nothrow) sf_op();
   if (!op) return SF_ERR_ARG;
@@ -542,7 +549,7 @@ int sf_create(sf_op** out, int D, int SB, int SQ, const double* A0, const double
       op->A_user[q * SB + j] = A0[q + SQ * j];  // column-major in
       op->B_user[q * SB + j] = B0[q + SQ * j];
     }
-  const int nloc = SB * SB * SB;
+  const int nloc = D == 2 ? SB * SB : SB * SB * SB;
   op->jt_user.resize(nloc * D);
   for (int k = 0; k < nloc; ++k)
     for (int d = 0; d < D; ++d) {
@@ -600,6 +607,8 @@ int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* 
                  int64_t n_free) {
   if (!op) return SF_ERR_ARG;
   return guarded(op, [&] {
+    SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED,
+               "D = 2 takes the structured Cartesian path (sf_set_structured) only");
     SF_REQUIRE(ncells >= 0 && n_free >= 0 && (ncells == 0 || (ptrs && data)), SF_ERR_ARG,
                "bad arguments to sf_set_cells");
     SF_REQUIRE(n_free < (1LL << 31), SF_ERR_ARG, "n_free must fit in int32");
@@ -639,8 +648,8 @@ int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* 
 int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_order) {
   if (!op) return SF_ERR_ARG;
   return guarded(op, [&] {
-    SF_REQUIRE(nx > 0 && ny > 0 && nz > 0 && node_order, SF_ERR_ARG,
-               "bad arguments to sf_set_structured");
+    SF_REQUIRE(nx > 0 && ny > 0 && (op->D == 2 ? nz == 0 : nz > 0) && node_order, SF_ERR_ARG,
+               "bad arguments to sf_set_structured (nz = 0 for D = 2)");
     std::vector<int> seen(op->SB, 0);
     for (int j = 0; j < op->SB; ++j) {
       SF_REQUIRE(node_order[j] >= 0 && node_order[j] < op->SB && !seen[node_order[j]], SF_ERR_ARG,
@@ -648,7 +657,7 @@ int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_ord
       seen[node_order[j]] = 1;
     }
     const long long p = op->p;
-    const long long fx = nx * p - 1, fy = ny * p - 1, fz = nz * p - 1;
+    const long long fx = nx * p - 1, fy = ny * p - 1, fz = op->D == 2 ? 1 : nz * p - 1;
     SF_REQUIRE(fx * fy * fz < (1LL << 31), SF_ERR_ARG, "mesh too large for int32 dof ids");
     for (int j = 0; j < op->SB; ++j) op->perm[j] = node_order[j];
     rebuild_kernel_basis(op);
@@ -656,7 +665,7 @@ int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_ord
     op->d_ids = nullptr;
     op->cells = sf::Cells();
     op->cells.mesh = sf::MESH_STRUCTURED;
-    op->cells.ncells = (long long)nx * ny * nz;
+    op->cells.ncells = (long long)nx * ny * (op->D == 2 ? 1 : nz);
     op->cells.nx = nx;
     op->cells.ny = ny;
     op->cells.nz = nz;
@@ -675,6 +684,7 @@ int sf_set_structured_slab(sf_op* op, int nx, int ny, int nz, int z0, int z1,
   const int status = sf_set_structured(op, nx, ny, z1 > z0 ? z1 - z0 : 1, node_order);
   if (status != SF_OK) return status;
   return guarded(op, [&] {
+    SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "slabs split a 3D mesh");
     SF_REQUIRE(nz > 0 && z0 >= 0 && z0 < z1 && z1 <= nz, SF_ERR_ARG,
                "slab cells [z0, z1) must lie in [0, nz) and be non-empty");
     const long long p = op->p;
@@ -697,7 +707,7 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
     SF_REQUIRE(fill || op->cells.mesh != sf::MESH_NONE, SF_ERR_STATE,
                "per-cell quantities need the mesh first (sf_set_cells / sf_set_structured)");
     const int SQ = op->SQ, D = op->D;
-    const int nq = SQ * SQ * SQ;
+    const int nq = D == 2 ? SQ * SQ : SQ * SQ * SQ;
     const long long nc = fill ? 1 : op->cells.ncells;
     // G = wq*djq*jq^T jq at every point (src/SumFactorizationKernels.jl:174-216)
     std::vector<double> G((size_t)nc * 6 * nq);
@@ -710,8 +720,9 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
         const double w = wq[(size_t)c * nq + q], dj = djq[(size_t)c * nq + q];
         WD[(size_t)c * nq + q] = w * dj;
         for (int m = 0; m < 6; ++m) {
-          double acc = 0.0;
-          for (int l = 0; l < D; ++l) acc += J[l + D * rr[m]] * J[l + D * kk[m]];
+          double acc = 0.0;  // in 2D the components with a z index stay zero
+          if (rr[m] < D && kk[m] < D)
+            for (int l = 0; l < D; ++l) acc += J[l + D * rr[m]] * J[l + D * kk[m]];
           H[((size_t)c * 6 + m) * nq + q] = dj * acc;
           G[((size_t)c * 6 + m) * nq + q] = w * dj * acc;
         }
@@ -728,6 +739,7 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
     bool sep = same;
     double Hmax = 0.0;
     for (int m = 0; m < 6; ++m) Hmax = std::max(Hmax, std::fabs(H[(size_t)m * nq]));
+    if (Hmax == 0.0) Hmax = 1.0;
     for (int m = 0; m < 6 && sep; ++m)
       for (int q = 1; q < nq; ++q)
         if (std::fabs(H[(size_t)m * nq + q] - H[(size_t)m * nq]) > 1e-13 * Hmax) {
@@ -739,12 +751,13 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
       const double w000 = wq[0];
       sep = w000 > 0;
       if (sep) {
-        const double c0 = std::cbrt(w000);
-        for (int i = 0; i < SQ; ++i) w1[i] = wq[i] / (c0 * c0);
-        for (int k = 0; k < SQ && sep; ++k)
+        // wq = w1 (x) w1 (x) w1 (D = 3) or w1 (x) w1 (D = 2), with w1[0] = c0
+        const double c0 = D == 2 ? std::sqrt(w000) : std::cbrt(w000);
+        for (int i = 0; i < SQ; ++i) w1[i] = wq[i] / (D == 2 ? c0 : c0 * c0);
+        for (int k = 0; k < (D == 2 ? 1 : SQ) && sep; ++k)
           for (int j = 0; j < SQ && sep; ++j)
             for (int i = 0; i < SQ; ++i) {
-              const double t = w1[i] * w1[j] * w1[k];
+              const double t = w1[i] * w1[j] * (D == 2 ? 1.0 : w1[k]);
               if (std::fabs(t - wq[i + SQ * (j + SQ * k)]) > 1e-13 * std::fabs(t)) {
                 sep = false;
                 break;
@@ -829,6 +842,7 @@ int sf_kappa_vjp(sf_op* op, int dtype, const void* x, const void* ybar, double* 
   return guarded(op, [&] {
     require_ready(op);
     SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_kappa_vjp does not take slab operators");
+    SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "sf_kappa_vjp is 3D only");
     SF_REQUIRE(x && ybar && kappa_bar, SF_ERR_ARG, "null x, ybar or kappa_bar");
     sf::launch_kappa_vjp(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, x,
                          ybar, kappa_bar, static_cast<cudaStream_t>(stream));
@@ -882,6 +896,7 @@ int sf_evaluate_cells(sf_op* op, int dtype, int64_t ncells, const void* x_cells,
   if (!op) return SF_ERR_ARG;
   return guarded(op, [&] {
     SF_REQUIRE(op->geom.kind != sf::GEOM_NONE, SF_ERR_STATE, "no geometry");
+    SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "sf_evaluate_cells is 3D only");
     SF_REQUIRE(ncells >= 0, SF_ERR_ARG, "ncells < 0");
     SF_REQUIRE(op->cq_cells <= 0 || op->cq_cells == ncells, SF_ERR_ARG,
                "ncells differs from the cell quantities");
@@ -901,6 +916,7 @@ int sf_rhs(sf_op* op, const double* fq, double* b, void* stream) {
     require_ready(op);
     SF_REQUIRE(fq && b, SF_ERR_ARG, "null fq or b");
     SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_rhs does not take slab operators");
+    SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "sf_rhs is 3D only");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     SF_CUDA_CHECK(cudaMemsetAsync(b, 0, op->n_free * sizeof(double), st));
     sf::launch_general_rhs(op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, fq, b,
@@ -915,8 +931,9 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream) {
     SF_REQUIRE(d, SF_ERR_ARG, "null d");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t es = dsize(dtype);
-    if (op->slab) {
-      SF_REQUIRE(dtype == SF_F64, SF_ERR_UNSUPPORTED, "the diagonal of a slab operator is FP64");
+    if (op->slab || op->D == 2) {
+      SF_REQUIRE(dtype == SF_F64, SF_ERR_UNSUPPORTED,
+                 "the diagonal of a slab or 2D operator is FP64");
       compute_diag(op, static_cast<double*>(d), st);
       return;
     }
@@ -1438,6 +1455,7 @@ extern "C" int sf_batch_create(sf_batch** out, int nops, sf_op* const* ops, int 
       sf_op* op = b->ops[i];
       SF_REQUIRE(op, SF_ERR_ARG, "null handle in the batch");
       require_ready(op);
+      SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "the batched form takes 3D operators");
       SF_REQUIRE(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64), SF_ERR_UNSUPPORTED,
                  "batch member " + std::to_string(i) +
                      " is not a constant-coefficient Cartesian problem (tiled kernel)");

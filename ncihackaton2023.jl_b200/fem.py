@@ -77,14 +77,15 @@ def lagrange_basis(nodes: np.ndarray, pts: np.ndarray):
     return A, B
 
 
-def hex_dof_map(p: int) -> np.ndarray:
+def hex_dof_map(p: int, D: int = 3) -> np.ndarray:
     """Tensor index (1-based, in the 1D Gridap basis order) of each local dof of
-    a hexahedron, as the (SB^3, 3) array m.dof_map of
-    src/SumFactorizationMaps.jl:40-45. The local order used by this package's
-    FE space is the tensor order with j1 fastest."""
+    a hexahedron (D = 3) or quadrilateral (D = 2), as the (SB^D, D) array
+    m.dof_map of src/SumFactorizationMaps.jl:40-45. The local order used by this
+    package's FE space is the tensor order with j1 fastest."""
     SB = p + 1
-    k = np.arange(SB ** 3)
-    return np.stack([k % SB, (k // SB) % SB, k // (SB * SB)], axis=1).astype(np.int32) + 1
+    k = np.arange(SB ** D)
+    cols = [k % SB, (k // SB) % SB, k // (SB * SB)][:D]
+    return np.stack(cols, axis=1).astype(np.int32) + 1
 
 
 # ----------------------------------------------------------------------------
@@ -105,7 +106,21 @@ class CartesianDiscreteModel:
     seed: int = 0
     vertices: np.ndarray = field(init=False, repr=False)
 
+    @property
+    def D(self) -> int:
+        return len(self.partition)
+
     def __post_init__(self):
+        if self.D == 2:
+            if len(self.domain) == 6:
+                self.domain = tuple(self.domain[:4])
+            if self.perturb > 0.0:
+                raise NotImplementedError("2D models are affine Cartesian (no perturbation)")
+            nx, ny = self.partition
+            X, Y = np.meshgrid(np.linspace(self.domain[0], self.domain[1], nx + 1),
+                               np.linspace(self.domain[2], self.domain[3], ny + 1), indexing="xy")
+            self.vertices = np.stack([X.ravel(), Y.ravel()], axis=1)
+            return
         nx, ny, nz = self.partition
         xs = [np.linspace(self.domain[2 * a], self.domain[2 * a + 1], n + 1)
               for a, n in enumerate(self.partition)]
@@ -131,7 +146,15 @@ class CartesianDiscreteModel:
         return self.perturb == 0.0
 
     def cell_vertices(self) -> np.ndarray:
-        """(ncells, 8) vertex ids, corners ordered with x fastest."""
+        """(ncells, 2^D) vertex ids, corners ordered with x fastest."""
+        if self.D == 2:
+            nx, ny = self.partition
+            c = np.arange(self.num_cells)
+            cx, cy = c % nx, c // nx
+            out = np.empty((self.num_cells, 4), dtype=np.int64)
+            for v in range(4):
+                out[:, v] = (cx + (v & 1)) + (nx + 1) * (cy + ((v >> 1) & 1))
+            return out
         nx, ny, nz = self.partition
         c = np.arange(self.num_cells)
         cx, cy, cz = c % nx, (c // nx) % ny, c // (nx * ny)
@@ -174,9 +197,8 @@ class FESpace:
         if self.dirichlet_tags != "boundary":
             raise NotImplementedError("only dirichlet_tags='boundary' is supported")
         p = self.order
-        nx, ny, nz = self.model.partition
-        self.grid = (nx * p + 1, ny * p + 1, nz * p + 1)
-        self.free_grid = (nx * p - 1, ny * p - 1, nz * p - 1)
+        self.grid = tuple(n * p + 1 for n in self.model.partition)
+        self.free_grid = tuple(n * p - 1 for n in self.model.partition)
         self._ids = None
         self.perm = None
         if self.renumber_seed is not None:
@@ -188,11 +210,13 @@ class FESpace:
         return int(np.prod(self.free_grid))
 
     def grid_ids(self) -> np.ndarray:
-        """Id of every point of the (N+1)^3 dof grid (x fastest): 1-based free ids,
+        """Id of every point of the (N+1)^D dof grid (x fastest): 1-based free ids,
         negative Dirichlet ids."""
-        Gx, Gy, Gz = self.grid
-        gz, gy, gx = np.meshgrid(np.arange(Gz), np.arange(Gy), np.arange(Gx), indexing="ij")
-        free = ((gx > 0) & (gx < Gx - 1) & (gy > 0) & (gy < Gy - 1) & (gz > 0) & (gz < Gz - 1)).ravel()
+        axes = np.meshgrid(*[np.arange(G) for G in self.grid[::-1]], indexing="ij")[::-1]
+        free = np.ones(axes[0].shape, dtype=bool)
+        for g, G in zip(axes, self.grid):
+            free &= (g > 0) & (g < G - 1)
+        free = free.ravel()
         ids = np.zeros(free.size, dtype=np.int64)
         lex = np.arange(1, int(free.sum()) + 1)
         if self.perm is not None:
@@ -203,6 +227,20 @@ class FESpace:
 
     def get_cell_dof_ids(self) -> Table:
         """The cell-to-dof Table in the local order of ``hex_dof_map(p)``."""
+        if self._ids is None and self.model.D == 2:
+            p, SB = self.order, self.order + 1
+            nx, ny = self.model.partition
+            Gx = self.grid[0]
+            gids = self.grid_ids()
+            c = np.arange(self.model.num_cells)
+            cx, cy = c % nx, c // nx
+            order = node_order(p)
+            dm = hex_dof_map(p, 2) - 1
+            ox, oy = order[dm[:, 0]], order[dm[:, 1]]
+            lin = (cx[:, None] * p + ox[None, :]) + Gx * (cy[:, None] * p + oy[None, :])
+            data = gids[lin].astype(np.int32).ravel()
+            ptrs = (np.arange(self.model.num_cells + 1, dtype=np.int64) * SB ** 2 + 1).astype(np.int32)
+            self._ids = Table(data=data, ptrs=ptrs)
         if self._ids is None:
             p = self.order
             SB = p + 1
@@ -223,6 +261,18 @@ class FESpace:
 
     def free_dof_coordinates(self) -> np.ndarray:
         """Coordinates of the free dofs in free-id order (unperturbed grid)."""
+        if self.model.D == 2:
+            fx, fy = self.free_grid
+            Gx, Gy = self.grid
+            gy, gx = np.meshgrid(np.arange(1, fy + 1), np.arange(1, fx + 1), indexing="ij")
+            d = self.model.domain
+            pts = np.stack([d[0] + (d[1] - d[0]) * gx.ravel() / (Gx - 1),
+                            d[2] + (d[3] - d[2]) * gy.ravel() / (Gy - 1)], axis=1)
+            if self.perm is not None:
+                out = np.empty_like(pts)
+                out[self.perm] = pts
+                return out
+            return pts
         fx, fy, fz = self.free_grid
         Gx, Gy, Gz = self.grid
         gz, gy, gx = np.meshgrid(np.arange(1, fz + 1), np.arange(1, fy + 1), np.arange(1, fx + 1),
@@ -283,6 +333,14 @@ def cell_quantities(model: CartesianDiscreteModel, q1d: np.ndarray, w1d: np.ndar
     arrays then hold one cell. jq is returned column-major per point
     (jq[..., l + 3 r] = jq[l, r]), the layout of the C ABI."""
     SQ = len(q1d)
+    if model.D == 2:  # affine Cartesian: Jt = diag(hx, hy) at every point
+        qy, qx = np.meshgrid(w1d, w1d, indexing="ij")
+        w = (qx * qy).ravel()
+        d = model.domain
+        hx, hy = (d[1] - d[0]) / model.partition[0], (d[3] - d[2]) / model.partition[1]
+        jq = np.tile(np.array([1.0 / hx, 0.0, 0.0, 1.0 / hy]), (1, SQ ** 2, 1))
+        djq = np.full((1, SQ ** 2), hx * hy)
+        return True, w[None, :].copy(), jq, djq
     qz, qy, qx = np.meshgrid(q1d, q1d, q1d, indexing="ij")
     pts = np.stack([qx.ravel(), qy.ravel(), qz.ravel()], axis=1)
     wz, wy, wx = np.meshgrid(w1d, w1d, w1d, indexing="ij")

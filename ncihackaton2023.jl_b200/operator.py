@@ -57,8 +57,8 @@ class SumFactorizationMap:
     def __init__(self, D: int, fe_orders, quad_orders):
         fe_orders = tuple(fe_orders)
         quad_orders = tuple(quad_orders)
-        if D != 3:
-            raise NotImplementedError("this build implements D = 3")
+        if D not in (2, 3):
+            raise NotImplementedError("this build implements D = 2 and D = 3")
         if len(set(fe_orders)) != 1 or len(set(quad_orders)) != 1:
             raise NotImplementedError("anisotropic orders are not supported (the reference's "
                                       "to_gpu(::SumFactorizationMap) is isotropic too)")
@@ -74,7 +74,7 @@ class SumFactorizationMap:
         self.points, self.weights = fem.gauss_legendre(nq)
         self.nodes = fem.lagrange_nodes(p)
         self.A0, self.B0 = fem.lagrange_basis(self.nodes, self.points)
-        self.dof_map = fem.hex_dof_map(p)
+        self.dof_map = fem.hex_dof_map(p, D)
         self.node_order = fem.node_order(p)
 
     @property
@@ -121,10 +121,12 @@ class LazyMatrix:
         self.gather = "table" if test.perm is not None else gather
         self._h = m._create_handle()
         try:
+            if m.D != self.model.D:
+                raise ValueError("the map's dimension differs from the model's")
             if self.gather == "structured":
-                nx, ny, nz = self.model.partition
+                part = tuple(self.model.partition) + ((0,) if m.D == 2 else ())
                 no = _i32(m.node_order)
-                check(lib.sf_set_structured(self._h, nx, ny, nz, _ptr(no)), self._h, "sf_set_structured")
+                check(lib.sf_set_structured(self._h, *part, _ptr(no)), self._h, "sf_set_structured")
             elif self.gather == "table":
                 t = test.get_cell_dof_ids()
                 ptrs, data = _i32(t.ptrs), _i32(t.data)

@@ -39,7 +39,8 @@ def test_host_only_calls(sf):
     assert lib.sf_cg(None, 0, None, None, 1e-10, 10, None, None, None) == _lib.SF_ERR_ARG
     out = C.c_void_p()
     # invalid arguments are rejected before any device work
-    assert lib.sf_create(C.byref(out), 2, 3, 3, None, None, None) == _lib.SF_ERR_UNSUPPORTED
+    assert lib.sf_create(C.byref(out), 4, 3, 3, None, None, None) == _lib.SF_ERR_UNSUPPORTED
+    assert lib.sf_create(C.byref(out), 2, 3, 3, None, None, None) == _lib.SF_ERR_ARG
     assert lib.sf_create(C.byref(out), 3, 11, 3, None, None, None) == _lib.SF_ERR_ARG
     assert lib.sf_create(None, 3, 3, 3, None, None, None) == _lib.SF_ERR_ARG
     assert out.value is None

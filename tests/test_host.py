@@ -22,7 +22,7 @@ def test_map_matches_oracle(sf, p, deg):
 
 def test_map_rejects_unsupported(sf):
     with pytest.raises(NotImplementedError):
-        sf.SumFactorizationMap(2, (2, 2), (4, 4))
+        sf.SumFactorizationMap(4, (2,) * 4, (4,) * 4)
     with pytest.raises(NotImplementedError):
         sf.SumFactorizationMap(3, (2, 3, 2), (4, 4, 4))
     with pytest.raises(ValueError):
