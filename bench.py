@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--cg-only", action="store_true",
                     help="only the CG solves (autotuned tiles; no apply leg): for profiling")
     ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
-    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8"], default=None,
+    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d"], default=None,
                     help="run only this secondary configuration (no apply leg): for profiling")
     ap.add_argument("--deformed-cells", type=int, default=32,
                     help="cells per direction of the deformed Q8 section")
@@ -306,7 +306,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
         return out
     if args.section is not None:
-        fn = {"batched": run_batched, "adjoint": run_adjoint,
+        fn = {"batched": run_batched, "adjoint": run_adjoint, "quad2d": run_quad2d,
               "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,
                                                             cg_iters=args.deformed_cg)}
         return {args.section: fn[args.section](sf, dev)}
@@ -409,7 +409,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_secondary and world == 1 and NCELL == 64:
         t_sec = time.perf_counter()
         for key, fn in (("batched", run_batched), ("adjoint", run_adjoint),
-                        ("deformed_q8", run_deformed)):
+                        ("deformed_q8", run_deformed), ("quad2d", run_quad2d)):
             if time.perf_counter() - t_sec > SECONDARY_BUDGET_S:
                 out[key] = {"skipped": "secondary time budget spent"}
                 continue
@@ -641,6 +641,51 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
         res[f"cg_{key}"] = {"s": round(time.perf_counter() - t0, 3), "iters": info["iters"],
                             "relres": info["relres"], "converged": info["converged"]}
     return res
+
+
+# The reference's only published timings (test/my_plot.jl:4-7): one 2D apply on
+# 1024 x 1024 cells, quadrature degree 2(p - 1), GPU sum-factorization kernel
+# gpu_mul_v3! on a V100 (its operator uses the weights only, no geometric factors).
+REF_2D_V100_S = {4: 0.003, 5: 0.0051, 6: 0.00805, 7: 0.014}
+
+
+def run_quad2d(sf, dev, n=1024, orders=(4, 5, 6, 7)):
+    """The reference's published 2D configuration on this GPU: 1024^2 cells, Q_p,
+    degree 2(p-1) quadrature, x ~ U[-1,1] (seed p), FP64 and FP32 applies of the full
+    Laplacian (with geometric factors), autotuned, 2 rotating x/y pairs."""
+    import torch
+    out = {"mesh": f"{n}^2 unit square", "reference_hw": "V100 (published, test/my_plot.jl)",
+           "note": "different hardware, and the reference's 2D kernel omits the geometric "
+                   "factors; the ratio is for orientation only"}
+    for p in orders:
+        deg = 2 * (p - 1)
+        model = sf.CartesianDiscreteModel((0, 1, 0, 1), (n, n))
+        V = sf.FESpace(model, p)
+        m = sf.SumFactorizationMap(2, (p, p), (deg, deg))
+        A = sf.LazyMatrix(m, V, V, sf.Measure(model, deg))
+        ndof = (n * p + 1) ** 2
+        rec = {"dofs": ndof}
+        for dt, key in ((torch.float64, "f64"), (torch.float32, "f32")):
+            A.autotune(dt)
+            rng = np.random.default_rng(p)
+            xs = [torch.from_numpy(rng.uniform(-1, 1, A.n)).to(dev, dt) for _ in range(2)]
+            ys = [torch.empty_like(xs[0]) for _ in range(2)]
+            for i in range(3):
+                sf.mul(ys[i % 2], A, xs[i % 2])
+            k = [0]
+
+            def step():
+                sf.mul(ys[k[0] % 2], A, xs[k[0] % 2])
+                k[0] += 1
+            ms = _events_ms(step, 20)
+            rec[key] = {"ms": round(ms, 4), "gdof_s": round(ndof / (ms * 1e-3) / 1e9, 2),
+                        "tile": A.kernel_name(dt)}
+        ref = REF_2D_V100_S.get(p)
+        if ref:
+            rec["reference_v100_ms"] = ref * 1e3
+            rec["ratio_vs_reference_v100_f64"] = round(ref * 1e3 / rec["f64"]["ms"], 1)
+        out[f"q{p}"] = rec
+    return out
 
 
 # ----------------------------------------------------------------------------
