@@ -54,7 +54,10 @@ const char* sf_status_string(int status);
  * Create an operator from the 1D data of a SumFactorizationMap.
  * Replaces SumFactorizationMap(D, fe_orders, quad_orders)
  * (src/SumFactorizationMaps.jl:47-65) plus to_gpu(m) (:25-32).
- *   D       : 3 (this build); 2 is rejected with SF_ERR_UNSUPPORTED
+ *   D       : 3, or 2 (quadrilaterals: structured Cartesian meshes only; the
+ *             table gather, evaluate_cells, kappa, rhs, slab and batched
+ *             forms return SF_ERR_UNSUPPORTED for D = 2). Other D:
+ *             SF_ERR_UNSUPPORTED
  *   SB, SQ  : 1D basis size p+1 (2..10) and quadrature size (1..10)
  *   A0, B0  : SQ x SB column-major, A0[i + SQ*j] = phi_j(xi_i), B0 = phi_j'(xi_i)
  *             (evalMats / B0 at src/SumFactorizationMaps.jl:53-54)
@@ -86,7 +89,8 @@ int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* 
 /*
  * Declare a Cartesian mesh: nx*ny*nz cells numbered with x fastest,
  * Dirichlet on the whole boundary, and free dofs numbered lexicographically
- * (x fastest) over the (nx*p-1) x (ny*p-1) x (nz*p-1) interior grid.
+ * (x fastest) over the (nx*p-1) x (ny*p-1) x (nz*p-1) interior grid. For an
+ * operator created with D = 2, pass nz = 0: nx*ny cells, (nx*p-1) x (ny*p-1) grid.
  * node_order[j] (0-based) is the position 0..p of 1D basis function j along
  * the segment; Gridap's order is {0, p, 1, 2, ..., p-1} (_get_terms,
  * src/SumFactorizationMaps.jl:34-38). This selects the tiled Cartesian kernels.
