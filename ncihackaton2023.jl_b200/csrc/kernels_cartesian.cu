@@ -543,17 +543,25 @@ k_cartesian2d(const __grid_constant__ CartParams2<P, T> Q) {
   const int tx = (int)blockIdx.x % Q.ntx, ty = (int)blockIdx.x / Q.ntx;
   const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1;
 
-  // pass 1: y segments (column x, cells sy*CY ..), inputs from global memory
+  // pass 1: y segments (column x, cells sy*CY ..), inputs from global memory; a tile
+  // whose input box lies inside the free grid needs no bounds checks
+  const bool interior = fx0 >= 0 && fy0 >= 0 && fx0 + G::BX <= Q.nfx && fy0 + G::BY <= Q.nfy;
   for (int w = threadIdx.x; w < G::BX * SY; w += NT) {
     const int x = w % G::BX, sy = w / G::BX;
     const int fx = fx0 + x, fyb = fy0 + sy * CY * P;
-    const bool inx = (unsigned)fx < (unsigned)Q.nfx;
     T c[NY];
+    if (interior) {
+      const T* col = Q.x + fx + (long long)Q.nfx * fyb;
 #pragma unroll
-    for (int i = 0; i < NY; ++i) {
-      const int fy = fyb + i;
-      c[i] = (inx && (unsigned)fy < (unsigned)Q.nfy) ? __ldg(Q.x + fx + (long long)Q.nfx * fy)
-                                                     : T(0);
+      for (int i = 0; i < NY; ++i) c[i] = __ldg(col + (long long)Q.nfx * i);
+    } else {
+      const bool inx = (unsigned)fx < (unsigned)Q.nfx;
+#pragma unroll
+      for (int i = 0; i < NY; ++i) {
+        const int fy = fyb + i;
+        c[i] = (inx && (unsigned)fy < (unsigned)Q.nfy) ? __ldg(Q.x + fx + (long long)Q.nfx * fy)
+                                                       : T(0);
+      }
     }
     seg_mk<P, CY, T>(Mm, Km, c, [&](int o, T m, T k) {
       const int yo = sy * CY * P + o;
@@ -896,7 +904,9 @@ struct Cands2;
 SF_C2(1, SF_T2D(1, 64, 64, 16, 16, 256, 2))
 SF_C2(2, SF_T2D(2, 32, 32, 8, 8, 256, 2))
 SF_C2(3, SF_T2D(3, 20, 20, 5, 5, 256, 2))
-SF_C2(4, SF_T2D(4, 16, 16, 4, 4, 256, 2), SF_T2D(4, 16, 16, 2, 4, 512, 1))
+SF_C2(4, SF_T2D(4, 16, 16, 4, 4, 256, 2), SF_T2D(4, 16, 16, 2, 4, 512, 1),
+      SF_T2D(4, 16, 16, 4, 4, 288, 2), SF_T2D(4, 16, 15, 4, 5, 256, 2),
+      SF_T2D(4, 20, 12, 5, 4, 256, 2))
 SF_C2(5, SF_T2D(5, 12, 12, 3, 3, 256, 2))
 SF_C2(6, SF_T2D(6, 10, 8, 2, 2, 256, 2))
 SF_C2(7, SF_T2D(7, 8, 8, 2, 2, 256, 2))
@@ -907,7 +917,9 @@ SF_C2(8, SF_T2D(8, 8, 8, 2, 2, 256, 2))
 SF_C2(1, SF_T2F(1, 64, 64, 16, 16, 256, 2))
 SF_C2(2, SF_T2F(2, 32, 32, 8, 8, 256, 2))
 SF_C2(3, SF_T2F(3, 20, 20, 5, 5, 256, 2))
-SF_C2(4, SF_T2F(4, 16, 16, 4, 4, 256, 2), SF_T2F(4, 16, 16, 2, 4, 512, 1))
+SF_C2(4, SF_T2F(4, 16, 16, 4, 4, 256, 2), SF_T2F(4, 16, 16, 2, 4, 512, 1),
+      SF_T2F(4, 16, 16, 4, 4, 288, 3), SF_T2F(4, 16, 15, 4, 5, 256, 3),
+      SF_T2F(4, 20, 12, 5, 4, 256, 3))
 SF_C2(5, SF_T2F(5, 12, 12, 3, 3, 256, 2))
 SF_C2(6, SF_T2F(6, 10, 8, 2, 2, 256, 2))
 SF_C2(7, SF_T2F(7, 8, 8, 2, 2, 256, 2))
