@@ -860,11 +860,19 @@ struct Candidate {
 // the operator's own mesh.
 template <int P, typename T>
 struct Cands;
-template <> struct Cands<1, double> { static constexpr Candidate c[] = {SF_TILE(1, double, 8, 8, 4, 256, 2)}; };
+// Low and high orders: tiles chosen so that the three passes (BX*BY columns, BX*OZ
+// and OY*OZ lines) keep most of the threads busy.
+template <> struct Cands<1, double> { static constexpr Candidate c[] = {SF_TILE(1, double, 8, 8, 4, 256, 2),
+                                                                      SF_TILE(1, double, 8, 16, 16, 256, 2),
+                                                                      SF_TILE(1, double, 16, 16, 16, 256, 2)}; };
 template <> struct Cands<2, double> { static constexpr Candidate c[] = {SF_TILE(2, double, 4, 4, 4, 256, 2),
-                                                                      SF_TILE(2, double, 8, 4, 2, 256, 2)}; };
+                                                                      SF_TILE(2, double, 8, 4, 2, 256, 2),
+                                                                      SF_TILE(2, double, 8, 8, 8, 256, 2),
+                                                                      SF_TILE(2, double, 4, 8, 8, 256, 2)}; };
 template <> struct Cands<3, double> { static constexpr Candidate c[] = {SF_TILE(3, double, 4, 4, 2, 256, 2),
-                                                                      SF_TILE(3, double, 4, 4, 3, 256, 2)}; };
+                                                                      SF_TILE(3, double, 4, 4, 3, 256, 2),
+                                                                      SF_TILE(3, double, 4, 6, 4, 256, 2),
+                                                                      SF_TILE(3, double, 4, 4, 6, 256, 2)}; };
 template <> struct Cands<4, double> { static constexpr Candidate c[] = {SF_TILE(4, double, 4, 4, 2, 256, 3),
                                                                       SF_TILE(4, double, 4, 4, 2, 256, 2),
                                                                       SF_TILE(4, double, 4, 4, 3, 256, 2),
@@ -873,22 +881,38 @@ template <> struct Cands<4, double> { static constexpr Candidate c[] = {SF_TILE(
                                                                       SF_TILE(4, double, 4, 4, 3, 320, 2),
                                                                       SF_TILE(4, double, 4, 4, 1, 128, 6),
                                                                       SF_TILE(4, double, 8, 4, 2, 256, 2)}; };
-template <> struct Cands<5, double> { static constexpr Candidate c[] = {SF_TILE(5, double, 2, 2, 2, 256, 2)}; };
-template <> struct Cands<6, double> { static constexpr Candidate c[] = {SF_TILE(6, double, 2, 2, 2, 256, 1)}; };
-template <> struct Cands<7, double> { static constexpr Candidate c[] = {SF_TILE(7, double, 2, 2, 1, 256, 1)}; };
-template <> struct Cands<8, double> { static constexpr Candidate c[] = {SF_TILE(8, double, 2, 2, 1, 256, 1)}; };
-template <> struct Cands<1, float> { static constexpr Candidate c[] = {SF_TILE(1, float, 8, 8, 4, 256, 2)}; };
-template <> struct Cands<2, float> { static constexpr Candidate c[] = {SF_TILE(2, float, 4, 4, 4, 256, 2)}; };
+template <> struct Cands<5, double> { static constexpr Candidate c[] = {SF_TILE(5, double, 2, 2, 2, 256, 2),
+                                                                      SF_TILE(5, double, 2, 3, 3, 256, 2),
+                                                                      SF_TILE(5, double, 2, 4, 2, 256, 2)}; };
+template <> struct Cands<6, double> { static constexpr Candidate c[] = {SF_TILE(6, double, 2, 2, 2, 256, 1),
+                                                                      SF_TILE(6, double, 2, 3, 2, 256, 2)}; };
+template <> struct Cands<7, double> { static constexpr Candidate c[] = {SF_TILE(7, double, 2, 2, 1, 256, 1),
+                                                                      SF_TILE(7, double, 2, 2, 2, 256, 1)}; };
+template <> struct Cands<8, double> { static constexpr Candidate c[] = {SF_TILE(8, double, 2, 2, 1, 256, 1),
+                                                                      SF_TILE(8, double, 2, 2, 2, 256, 1)}; };
+template <> struct Cands<1, float> { static constexpr Candidate c[] = {SF_TILE(1, float, 8, 8, 4, 256, 2),
+                                                                     SF_TILE(1, float, 8, 16, 16, 256, 3),
+                                                                     SF_TILE(1, float, 16, 16, 16, 256, 2)}; };
+template <> struct Cands<2, float> { static constexpr Candidate c[] = {SF_TILE(2, float, 4, 4, 4, 256, 2),
+                                                                     SF_TILE(2, float, 8, 8, 8, 256, 2),
+                                                                     SF_TILE(2, float, 4, 8, 8, 256, 3)}; };
 template <> struct Cands<3, float> { static constexpr Candidate c[] = {SF_TILE(3, float, 4, 4, 4, 256, 2),
-                                                                     SF_TILE(3, float, 4, 4, 2, 256, 3)}; };
+                                                                     SF_TILE(3, float, 4, 4, 2, 256, 3),
+                                                                     SF_TILE(3, float, 4, 6, 4, 256, 2),
+                                                                     SF_TILE(3, float, 4, 4, 6, 256, 2)}; };
 template <> struct Cands<4, float> { static constexpr Candidate c[] = {SF_TILE(4, float, 4, 4, 2, 256, 3),
                                                                      SF_TILE(4, float, 4, 4, 3, 256, 3),
                                                                      SF_TILE(4, float, 4, 4, 4, 256, 3),
                                                                      SF_TILE(4, float, 4, 4, 3, 256, 4)}; };
-template <> struct Cands<5, float> { static constexpr Candidate c[] = {SF_TILE(5, float, 2, 2, 2, 256, 2)}; };
-template <> struct Cands<6, float> { static constexpr Candidate c[] = {SF_TILE(6, float, 2, 2, 2, 256, 2)}; };
-template <> struct Cands<7, float> { static constexpr Candidate c[] = {SF_TILE(7, float, 2, 2, 2, 256, 2)}; };
-template <> struct Cands<8, float> { static constexpr Candidate c[] = {SF_TILE(8, float, 2, 2, 1, 256, 2)}; };
+template <> struct Cands<5, float> { static constexpr Candidate c[] = {SF_TILE(5, float, 2, 2, 2, 256, 2),
+                                                                     SF_TILE(5, float, 2, 3, 3, 256, 2),
+                                                                     SF_TILE(5, float, 2, 4, 2, 256, 2)}; };
+template <> struct Cands<6, float> { static constexpr Candidate c[] = {SF_TILE(6, float, 2, 2, 2, 256, 2),
+                                                                     SF_TILE(6, float, 2, 3, 2, 256, 2)}; };
+template <> struct Cands<7, float> { static constexpr Candidate c[] = {SF_TILE(7, float, 2, 2, 2, 256, 2),
+                                                                     SF_TILE(7, float, 2, 2, 1, 256, 2)}; };
+template <> struct Cands<8, float> { static constexpr Candidate c[] = {SF_TILE(8, float, 2, 2, 1, 256, 2),
+                                                                     SF_TILE(8, float, 2, 2, 2, 256, 1)}; };
 #undef SF_TILE
 
 // 2D candidates: tiles of about 64 x 64 points; pass 2 gives every thread one x segment.
