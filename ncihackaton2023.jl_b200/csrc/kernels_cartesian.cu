@@ -188,8 +188,12 @@ struct Tile {
   // request that wraps from one z-plane into the next then maps onto the banks as
   // if the rows were contiguous, so it has no bank conflicts.
   static constexpr int M = sizeof(T) == 8 ? 16 : 32;
-  static constexpr int PAD = ((BX - BX * BY) % M + M) % M;
-  static constexpr int PLANE = BX * BY + PAD;
+  // Rows inside a plane have an odd pitch RX: the x pass gives consecutive threads
+  // consecutive rows, and an even pitch (BX = 16 at p = 3 or 5 with small tiles)
+  // would put their accesses on the same banks.
+  static constexpr int RX = BX | 1;
+  static constexpr int PAD = ((BX - RX * BY) % M + M) % M;
+  static constexpr int PLANE = RX * BY + PAD;
   static constexpr int TS = PLANE * OZ;  // each of t1 (-> a -> y) and t2 (-> s)
   static constexpr int WORDS = 2 * TS;
 };
@@ -291,6 +295,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     }
   };
   auto z_line = [&](int l, const T (&c)[G::BZ]) {
+    const int sl = G::RX == G::BX ? l : (l % G::BX) + G::RX * (l / G::BX);  // in-plane offset
     T cm = T(0), ck = T(0);
 #pragma unroll
     for (int k = 0; k < EZ; ++k) {
@@ -304,15 +309,15 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
       mac<P, T>(Mm, s, am.e, am.o);
       mac<P, T>(Km, s, ak.e, ak.o);
       if (k > 0) {
-        T1[(k * P - 1) * G::PLANE + l] = am.at(0) + cm;
+        T1[(k * P - 1) * G::PLANE + sl] = am.at(0) + cm;
         const T v = ak.at(0) + ck;
-        T2[(k * P - 1) * G::PLANE + l] = ISO ? v : v * rz;
+        T2[(k * P - 1) * G::PLANE + sl] = ISO ? v : v * rz;
       }
 #pragma unroll
       for (int m = 1; m < P; ++m) {
-        T1[(k * P + m - 1) * G::PLANE + l] = am.at(m);
+        T1[(k * P + m - 1) * G::PLANE + sl] = am.at(m);
         const T v = ak.at(m);
-        T2[(k * P + m - 1) * G::PLANE + l] = ISO ? v : v * rz;
+        T2[(k * P + m - 1) * G::PLANE + sl] = ISO ? v : v * rz;
       }
       cm = am.at(P);
       ck = ak.at(P);
@@ -321,9 +326,9 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
 #pragma unroll
     for (int m = 0; m <= P; ++m) u[m] = c[EZ * P + m];
     const Split<P, T> s = split<P, T>(u);
-    T1[(EZ * P - 1) * G::PLANE + l] = mac_row0<P, T>(Mm, s, cm);
+    T1[(EZ * P - 1) * G::PLANE + sl] = mac_row0<P, T>(Mm, s, cm);
     const T v = mac_row0<P, T>(Km, s, ck);
-    T2[(EZ * P - 1) * G::PLANE + l] = ISO ? v : v * rz;
+    T2[(EZ * P - 1) * G::PLANE + sl] = ISO ? v : v * rz;
   };
   constexpr int ZL = G::BX * G::BY;
   if constexpr (ZL > NT && ZL <= 2 * NT) {
@@ -348,7 +353,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     const int x = l % G::BX, zo = l / G::BX;
     T* const ln[2] = {T1 + zo * G::PLANE + x, T2 + zo * G::PLANE + x};
     smem_line<P, EY, 2, 2, T>(
-        ln, G::BX,
+        ln, G::RX,
         [&](const Split<P, T>(&s)[2], Acc<P, T>(&acc)[2]) {
           mac<P, T>(Mm, s[0], acc[0].e, acc[0].o);
           mac<P, T>(Km, s[0], acc[1].e, acc[1].o);
@@ -365,7 +370,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   // ---- x pass: lines (yo, zo): y = cy (K a + M s) -> T1 ----
   for (int l = threadIdx.x; l < G::OY * G::OZ; l += NT) {
     const int yo = l % G::OY, zo = l / G::OY;
-    T* const ln[2] = {T1 + zo * G::PLANE + yo * G::BX, T2 + zo * G::PLANE + yo * G::BX};
+    T* const ln[2] = {T1 + zo * G::PLANE + yo * G::RX, T2 + zo * G::PLANE + yo * G::RX};
     smem_line<P, EX, 2, 1, T>(
         ln, 1,
         [&](const Split<P, T>(&s)[2], Acc<P, T>(&acc)[1]) {
@@ -391,7 +396,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     const int yo = r % G::OY;
     const int zo = r / G::OY;
     o = xo + (long long)nfx * (yo + (long long)nfy * zo);
-    t1 = zo * G::PLANE + yo * G::BX + xo;
+    t1 = zo * G::PLANE + yo * G::RX + xo;
     return full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz_out);
   };
   if (!dot) {
