@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -333,15 +334,22 @@ struct Report {
   double rr, done, iters;
 };
 
-// Waits for report number k (or a later one) and returns it.
+// Waits for report number k (or a later one) and returns it. Gives up with an
+// error if the stream ends or fails without it, or after kReportWaitSeconds.
+constexpr double kReportWaitSeconds = 600.0;
+
 Report wait_report(sf_op* op, int k, cudaStream_t st) {
   volatile const double* r = op->h_report;
+  const auto t0 = std::chrono::steady_clock::now();
   for (unsigned spin = 1; r[3] < k; ++spin) {
     if ((spin & 255) == 0) {
       const cudaError_t e = cudaStreamQuery(st);
       if (e == cudaSuccess && r[3] < k)
         throw Error(SF_ERR_STATE, "CG progress report missing");
       if (e != cudaSuccess && e != cudaErrorNotReady) SF_CUDA_CHECK(e);
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >
+          kReportWaitSeconds)
+        throw Error(SF_ERR_CUDA, "no CG progress from the device within the wait limit");
       std::this_thread::yield();
     }
   }
