@@ -61,3 +61,32 @@ def test_missing_library_fails_loudly(tmp_path):
             "sys.modules['p']=m;s.loader.exec_module(m)")
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
     assert r.returncode != 0 and "ImportError" in r.stderr and "libsfb200.so" in r.stderr
+
+
+def test_null_handles_are_rejected(sf):
+    """Every entry point that takes a handle answers SF_ERR_ARG for a null one,
+    without touching a device."""
+    from ncihackaton2023_b200 import _lib
+    lib = _lib.lib
+    ARG = _lib.SF_ERR_ARG
+    assert lib.sf_rhs(None, None, None, None) == ARG
+    assert lib.sf_set_structured_slab(None, 2, 2, 4, 0, 2, None) == ARG
+    assert lib.sf_cgd_start(None, None, None, None, None, None, None, None) == ARG
+    assert lib.sf_cgd_init(None, None, 1e-10, None) == ARG
+    assert lib.sf_cgd_apply(None, None, None, None, None) == ARG
+    assert lib.sf_cgd_update(None, None, None, None, None) == ARG
+    assert lib.sf_cgd_direction(None, None, None, None, None, None) == ARG
+    assert lib.sf_set_structured(None, 2, 2, 2, None) == ARG
+    assert lib.sf_mul_host(None, None, None) == ARG
+    assert lib.sf_diagonal(None, 0, None, None) == ARG
+    assert lib.sf_autotune(None, 0, None) == ARG
+    assert lib.sf_kappa_vjp(None, 0, None, None, None, None) == ARG
+
+
+def test_scalar_block_layout_matches_the_header(sf):
+    """The distributed CG's scalar slots as the header documents them."""
+    from ncihackaton2023_b200 import _lib
+    text = open(HEADER).read()
+    for name in ("SF_CGD_SCALARS", "SF_CGD_RR", "SF_CGD_BB", "SF_CGD_DONE", "SF_CGD_ITERS"):
+        m = re.search(r"#define\s+" + name + r"\s+(\d+)", text)
+        assert m and int(m.group(1)) == getattr(_lib, name), name
