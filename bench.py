@@ -435,7 +435,7 @@ SECONDARY_BUDGET_S = 180.0
 def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
     import torch
     res, sols = {}, {}
-    for mode in ("jacobi", "mixed"):
+    for mode in ("jacobi", "mixed", "plain"):
         if warm:  # workspaces, diagonal
             sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=maxiter, raise_on_fail=False)
         torch.cuda.synchronize()
@@ -446,7 +446,7 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
             e1.record()
             torch.cuda.synchronize()
         sols[mode] = x
-        key = "f64" if mode == "jacobi" else "mixed"
+        key = {"jacobi": "f64", "mixed": "mixed", "plain": "f64_plain"}[mode]
         ms = e0.elapsed_time(e1)
         res[key] = {"ms": round(ms, 3), "iters": info["iters"],
                     "ms_per_iter": round(ms / max(1, info["iters"]), 4),
@@ -458,6 +458,7 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
     res["mixed"]["err_vs_f64_max_rel"] = ((sols["mixed"] - sols["jacobi"]).abs().max() /
                                           sols["jacobi"].abs().max()).item()
     res["speedup_mixed_vs_f64"] = round(res["f64"]["ms"] / res["mixed"]["ms"], 3)
+    res["speedup_mixed_vs_f64_plain"] = round(res["f64_plain"]["ms"] / res["mixed"]["ms"], 3)
     return res
 
 
@@ -465,8 +466,9 @@ def run_cg(sf, m, model, V, A, dev, maxiter=CG_MAXITER):
     """CG to relres 1e-10: the manufactured problem of the benchmark
     (f = 3 pi^2 sin sin sin; its right-hand side formed on the device by sf_rhs,
     and on the host by numpy as a cross-check), and a rough right-hand side
-    (b ~ U[-1,1], seed 1), both FP64 Jacobi CG and mixed precision (FP32
-    recurrence and apply, FP64 reliable updates)."""
+    (b ~ U[-1,1], seed 1): FP64 Jacobi CG, mixed precision (FP32 recurrence and
+    apply with Jacobi, FP64 reliable updates), and FP64 CG without a
+    preconditioner (the reference's cg! call, profiling/drivers.jl:87)."""
     import torch
 
     def f(X):  # f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z) at (..., 3) device coordinates
