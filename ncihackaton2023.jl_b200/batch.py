@@ -88,3 +88,28 @@ class Batch:
 def column_major(n: int, nrhs: int, dtype=torch.float64, device="cuda"):
     """An (n, nrhs) column-major tensor (its transpose is contiguous)."""
     return torch.empty(nrhs, n, dtype=dtype, device=device).t()
+
+
+def apply_cost(n_cells: int, p: int, nrhs: int = 1) -> float:
+    """Work estimate of one problem's batched apply: its dofs times an order factor
+    (the tiled kernel's FP64 time per dof grows with p, roughly like (p + 1)),
+    times the right-hand sides."""
+    return float(n_cells) * p ** 3 * (p + 1) * nrhs
+
+
+def shard(costs, nranks: int) -> list[list[int]]:
+    """Indices of independent problems dealt to ``nranks`` ranks, balanced by cost:
+    largest first, each to the currently lightest rank (ties: lowest rank). The
+    problems share nothing, so each rank then runs its own Batch with no exchange.
+    Deterministic, so every rank computes the same assignment."""
+    if nranks < 1:
+        raise ValueError("nranks must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * nranks
+    out: list[list[int]] = [[] for _ in range(nranks)]
+    for i in order:
+        r = min(range(nranks), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(o) for o in out]
+

@@ -175,3 +175,21 @@ def test_gloo_two_ranks_match_oracle(sf, tmp_path):
     assert not np.isnan(y).any() and not np.isnan(x).any()
     assert np.abs(y - S @ xg).max() <= 1e-13 * np.abs(S @ xg).max()
     assert np.abs(x - x_ref).max() < 1e-8 * np.abs(x_ref).max()
+
+
+def test_batched_problems_shard_by_cost(sf):
+    """The batched form's independent problems are dealt to ranks by a greedy
+    cost balance (no exchange between ranks); every rank gets the same answer."""
+    shard, cost = sf.batch.shard, sf.batch.apply_cost
+    rng = np.random.default_rng(2024)
+    specs = [(int(rng.integers(8, 41)), int(rng.integers(2, 7))) for _ in range(48)]
+    costs = [cost(n ** 3, p, 4) for n, p in specs]
+    for nranks in (1, 2, 3, 8):
+        parts = shard(costs, nranks)
+        assert sorted(i for part in parts for i in part) == list(range(48))
+        loads = [sum(costs[i] for i in part) for part in parts]
+        # greedy largest-first: no rank exceeds the mean by more than the largest problem
+        assert max(loads) <= sum(costs) / nranks + max(costs)
+        assert parts == shard(costs, nranks)
+    with pytest.raises(ValueError):
+        shard(costs, 0)
