@@ -210,6 +210,7 @@ def run_slabs(args, sf, rank, world, dev):
     D = sf.distributed.DistributedLazyMatrix(m, model, nparts=world, group=dist.group.WORLD,
                                              device=dev)
     D.autotune(torch.float64)
+    dist.barrier()  # the world communicator exists before the first point-to-point exchange
     L = D.layouts[0]
     n_total = (NCELL * P + 1) ** 2 * (nz * P + 1)
     rng = np.random.default_rng(rank)
