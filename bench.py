@@ -436,18 +436,25 @@ SECONDARY_BUDGET_S = 180.0
 def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
     import torch
     res, sols = {}, {}
-    for mode in ("jacobi", "mixed", "plain"):
+    fused = A.info("cg_fused") == 1.0
+    # "jacobi_unfused": the same FP64 Jacobi CG with the apply and vector kernels
+    # as separate launches (for comparison with the fused iteration)
+    for mode in ("jacobi", "mixed", "plain") + (("jacobi_unfused",) if fused else ()):
+        A.set_option("cg_fused", 0 if mode == "jacobi_unfused" else 1)
+        cg_mode = "jacobi" if mode == "jacobi_unfused" else mode
         if warm:  # workspaces, diagonal
-            sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=maxiter, raise_on_fail=False)
+            sf.cg(A, b, reltol=1e-10, mode=cg_mode, maxiter=maxiter, raise_on_fail=False)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(torch.cuda.current_device()) as clk:
             e0.record()
-            x, info = sf.cg(A, b, reltol=1e-10, mode=mode, maxiter=maxiter, raise_on_fail=False)
+            x, info = sf.cg(A, b, reltol=1e-10, mode=cg_mode, maxiter=maxiter,
+                            raise_on_fail=False)
             e1.record()
             torch.cuda.synchronize()
         sols[mode] = x
-        key = {"jacobi": "f64", "mixed": "mixed", "plain": "f64_plain"}[mode]
+        key = {"jacobi": "f64", "mixed": "mixed", "plain": "f64_plain",
+               "jacobi_unfused": "f64_unfused"}[mode]
         ms = e0.elapsed_time(e1)
         res[key] = {"ms": round(ms, 3), "iters": info["iters"],
                     "ms_per_iter": round(ms / max(1, info["iters"]), 4),
@@ -456,8 +463,14 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
         log(f"cg {key}: {res[key]}")
         if u_exact is not None:
             res[key]["err_vs_exact_max"] = (x - u_exact).abs().max().item()
+    A.set_option("cg_fused", 1)
+    res["f64"]["iteration"] = A.cg_kernel_name()
     res["mixed"]["err_vs_f64_max_rel"] = ((sols["mixed"] - sols["jacobi"]).abs().max() /
                                           sols["jacobi"].abs().max()).item()
+    if "jacobi_unfused" in sols:
+        res["f64_unfused"]["err_vs_f64_max_rel"] = (
+            (sols["jacobi_unfused"] - sols["jacobi"]).abs().max() / sols["jacobi"].abs().max()).item()
+        res["speedup_fused_vs_unfused"] = round(res["f64_unfused"]["ms"] / res["f64"]["ms"], 3)
     res["speedup_mixed_vs_f64"] = round(res["f64"]["ms"] / res["mixed"]["ms"], 3)
     res["speedup_mixed_vs_f64_plain"] = round(res["f64_plain"]["ms"] / res["mixed"]["ms"], 3)
     return res

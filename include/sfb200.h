@@ -197,6 +197,12 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream);
  * at profiling/drivers.jl:85-95. Stops when ||r||_2 <= reltol * ||b||_2
  * (FP64 true residual for SF_CG_MIXED). Reports iterations (FP32 iterations
  * for SF_CG_MIXED) and the final relative residual.
+ * On a whole 3D Cartesian mesh of order 1..8 (the tiled kernel in use), the
+ * FP64 modes run one fused kernel per iteration: the vector updates of
+ * iteration k-1 (x, r, and the next direction p) and q = A p in one sweep,
+ * with the Jacobi diagonal taken from a per-cell-position table (option
+ * "cg_fused" = 0 selects the unfused iteration: the apply and two vector
+ * kernels). Both are the same CG; iteration counts agree within one.
  */
 int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter,
           int* iters, double* relres, void* stream);
@@ -241,6 +247,9 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *                          dropped by this factor (default 0.1)
  *   "tile_candidate_f64"  : force tile-shape candidate k of the tiled Cartesian kernel
  *   "tile_candidate_f32"    (0-based; see sf_get_info "tile_candidates_f64/f32")
+ *   "cg_fused"            : 1 (default) fused FP64 CG iteration where available, 0 unfused
+ *   "cg_candidate"        : force tile-shape candidate k of the fused CG kernel
+ *                           (0-based; see sf_get_info "cg_candidates")
  */
 int sf_set_option(sf_op* op, const char* name, double value);
 
@@ -258,13 +267,16 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *   "plane_size"             : free points per z-level (structured meshes)
  *   "owned_offset", "owned_count": the points sf_apply writes (the whole vector
  *                              unless the operator is a slab)
+ *   "cg_fused"               : 1 if sf_cg's FP64 modes use the fused CG kernel
+ *   "cg_candidates"          : number of tile shapes of the fused CG kernel
  */
 int sf_get_info(const sf_op* op, const char* key, double* value);
 
 /*
  * Time every tile-shape candidate of the tiled Cartesian kernel for this
  * handle's order, mesh and dtype, and keep the fastest for later sf_apply
- * calls. Temporary x / y buffers are allocated for the timing. Without the
+ * calls; for SF_F64 also the fused CG kernel's candidates, for later sf_cg
+ * calls. Temporary vectors are allocated for the timing. Without the
  * tiled kernel (table gather, deformed cells, kappa) it does nothing.
  * Replaces the launch-configuration table that the reference kept by hand
  * (test/benchmark_v3.jl:36-40).
@@ -273,6 +285,9 @@ int sf_autotune(sf_op* op, int dtype, void* stream);
 
 /* Description of the kernel sf_apply uses for dtype (static string). */
 const char* sf_kernel_name(const sf_op* op, int dtype);
+
+/* Description of the iteration sf_cg's FP64 modes run (static string). */
+const char* sf_cg_kernel_name(const sf_op* op);
 
 /*
  * Batched form: many independent Cartesian problems (handles on which the

@@ -73,6 +73,7 @@ SIGNATURES = {
     "sf_batch_autotune": (i32, [vp, i32, C.POINTER(vp), C.POINTER(vp), vp]),
     "sf_batch_group_kernel": (C.c_char_p, [vp, i32, i32]),
     "sf_kernel_name": (C.c_char_p, [vp, i32]),
+    "sf_cg_kernel_name": (C.c_char_p, [vp]),
     "sf_set_structured_slab": (i32, [vp, i32, i32, i32, i32, i32, vp]),
     "sf_rhs": (i32, [vp, vp, vp, vp]),
     "sf_cgd_start": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),

@@ -253,47 +253,18 @@ __device__ __forceinline__ void smem_line(T* const (&ln)[2], int st, const Body&
   for (int j = 0; j < NOUT; ++j) ln[j][(E * P - 1) * st] = fin(j, r[j] + carry[j]);
 }
 
-// One output tile: cells [tx*EX, (tx+1)*EX) x [ty*EY, ...) x [tz*EZ, ...) of a free grid
-// nfx x nfy x nfz. Inputs outside the free grid read as zero, except that the
-// z range read is [zlo, nfz) (zlo = -1: a slab's halo plane below it); outputs
-// are written for z < nfz_out. T1/T2: shared buffers of Tile::TS words each. Ends with the
-// outputs stored; the caller synchronises before reusing T1/T2. With `dot`
-// non-null, *dot receives the FP64 sum of x*y over the tile's outputs (the
-// (p, A p) term of CG), summed in a fixed order.
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T>
-__device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
-                                          const EOMat<P, T>& Km, const T* __restrict__ X,
-                                          T* __restrict__ Y, int nfx, int nfy, int nfz, int zlo,
-                                          int nfz_out, int tx,
-                                          int ty, int tz, T rz, T rx, T cy,
-                                          double* dot = nullptr) {
+// The three line passes of one tile. load_col(l, c) fills c with input z-column
+// l of the tile's input box (x = l % BX, y = l / BX; points 0 .. BZ-1 along z).
+// On return T1 holds the tile's outputs (plane stride PLANE, row pitch RX) and
+// every thread has passed a barrier after the last pass. PAIR: when the box has
+// between NT and 2 NT columns, a thread loads both of its columns before it
+// computes either.
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, bool PAIR, typename T, typename Load>
+__device__ __forceinline__ void tile_passes(T* T1, T* T2, const EOMat<P, T>& Mm,
+                                            const EOMat<P, T>& Km, T rz, T rx, T cy,
+                                            const Load& load_col) {
   using G = Tile<P, EX, EY, EZ, T>;
-  // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
-  const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
-  const long long pz = (long long)nfx * nfy;
-
-  // a tile whose whole input box lies inside the free grid needs no bounds checks
-  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= zlo && fx0 + G::BX <= nfx &&
-                        fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
-
-  // ---- z pass: one z-line per thread, read from global memory ----
-  auto load_col = [&](int l, T (&c)[G::BZ]) {
-    const int x = l % G::BX, y = l / G::BX;
-    const int fx = fx0 + x, fy = fy0 + y;
-    if (interior) {
-      const T* col = X + (long long)fx + (long long)nfx * fy + fz0 * pz;
-#pragma unroll
-      for (int z = 0; z < G::BZ; ++z) c[z] = __ldg(col + z * pz);
-    } else {
-      const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
-      const T* col = X + (long long)fx + (long long)nfx * fy;
-#pragma unroll
-      for (int z = 0; z < G::BZ; ++z) {
-        const int fz = fz0 + z;
-        c[z] = (inxy && (unsigned)(fz - zlo) < (unsigned)(nfz - zlo)) ? __ldg(col + fz * pz) : T(0);
-      }
-    }
-  };
+  // ---- z pass: one z-line per thread, inputs from load_col ----
   auto z_line = [&](int l, const T (&c)[G::BZ]) {
     const int sl = G::RX == G::BX ? l : (l % G::BX) + G::RX * (l / G::BX);  // in-plane offset
     T cm = T(0), ck = T(0);
@@ -331,7 +302,7 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     T2[(EZ * P - 1) * G::PLANE + sl] = ISO ? v : v * rz;
   };
   constexpr int ZL = G::BX * G::BY;
-  if constexpr (ZL > NT && ZL <= 2 * NT) {
+  if constexpr (PAIR && ZL > NT && ZL <= 2 * NT) {
     // two z-lines per thread: both columns' loads are in flight before either computes
     const int l0 = threadIdx.x, l1 = threadIdx.x + NT;
     T c0[G::BZ], c1[G::BZ];
@@ -383,6 +354,49 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
         [&](int, T v) { return v * cy; });
   }
   __syncthreads();
+}
+
+// One output tile: cells [tx*EX, (tx+1)*EX) x [ty*EY, ...) x [tz*EZ, ...) of a free grid
+// nfx x nfy x nfz. Inputs outside the free grid read as zero, except that the
+// z range read is [zlo, nfz) (zlo = -1: a slab's halo plane below it); outputs
+// are written for z < nfz_out. T1/T2: shared buffers of Tile::TS words each. Ends with the
+// outputs stored; the caller synchronises before reusing T1/T2. With `dot`
+// non-null, *dot receives the FP64 sum of x*y over the tile's outputs (the
+// (p, A p) term of CG), summed in a fixed order.
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T>
+__device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
+                                          const EOMat<P, T>& Km, const T* __restrict__ X,
+                                          T* __restrict__ Y, int nfx, int nfy, int nfz, int zlo,
+                                          int nfz_out, int tx,
+                                          int ty, int tz, T rz, T rx, T cy,
+                                          double* dot = nullptr) {
+  using G = Tile<P, EX, EY, EZ, T>;
+  // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
+  const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
+  const long long pz = (long long)nfx * nfy;
+
+  // a tile whose whole input box lies inside the free grid needs no bounds checks
+  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= zlo && fx0 + G::BX <= nfx &&
+                        fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
+
+  auto load_col = [&](int l, T (&c)[G::BZ]) {
+    const int x = l % G::BX, y = l / G::BX;
+    const int fx = fx0 + x, fy = fy0 + y;
+    if (interior) {
+      const T* col = X + (long long)fx + (long long)nfx * fy + fz0 * pz;
+#pragma unroll
+      for (int z = 0; z < G::BZ; ++z) c[z] = __ldg(col + z * pz);
+    } else {
+      const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
+      const T* col = X + (long long)fx + (long long)nfx * fy;
+#pragma unroll
+      for (int z = 0; z < G::BZ; ++z) {
+        const int fz = fz0 + z;
+        c[z] = (inxy && (unsigned)(fz - zlo) < (unsigned)(nfz - zlo)) ? __ldg(col + fz * pz) : T(0);
+      }
+    }
+  };
+  tile_passes<P, EX, EY, EZ, NT, ISO, true, T>(T1, T2, Mm, Km, rz, rx, cy, load_col);
 
   // ---- store the owned outputs (free coords start at e0*p) ----
   const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
@@ -431,6 +445,193 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   }
   const double t = cta_sum<NT>(acc);  // the same branch in every thread of the CTA
   if (threadIdx.x == 0) *dot = t;
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused FP64 CG pass on the Cartesian operator. One launch carries iteration k
+// of the CG that profiling/drivers.jl:85-95 runs (Jacobi-preconditioned or plain):
+//   r_k = r_{k-1} - alpha q_{k-1},   x_k = x_{k-1} + alpha p_{k-1},
+//   p_k = D^-1 r_k + beta p_{k-1},   q_k = A p_k,
+// with alpha = alpha_{k-1} and beta = beta_{k-1} from the device scalars (both 0
+// on the first pass, which then forms p_0 = D^-1 r_0 and q_0 only). A tile forms
+// p_k on its whole input box, halo included, from the k-1 vectors, and writes
+// x, r and p on its owned points only. The k-1 vectors (r, q, p) are therefore
+// other buffers than the k ones; the caller alternates two sets. A tile
+// computes a halo value with the same operations as the value's owner, so A is
+// applied to exactly the p that is stored.
+// On a Cartesian mesh D^-1 depends only on the position of a point inside its
+// cell (the assembled 1D diagonals repeat with period p), so it comes from a
+// p^3 table in shared memory, not from a vector (all ones for the plain CG).
+// Per tile, in a fixed order, the pass sums
+//   (p_k, q_k), (r_k, D^-1 r_k), (r_k, r_k), (r_k, D^-1 q_k), (q_k, D^-1 q_k).
+// From them the one-block step after the pass forms alpha_k, the stopping test
+// on (r_k, r_k), and beta_k, with (r_{k+1}, D^-1 r_{k+1}) taken one step ahead by
+//   (r - a q, D^-1 (r - a q)) = (r, D^-1 r) - 2a (r, D^-1 q) + a^2 (q, D^-1 q).
+// The exact (r_k, D^-1 r_k) of every pass restarts that recurrence, so its
+// rounding does not build up over the iterations.
+// Memory traffic per pass: r, q, p read on the box, x read on the owned points,
+// x, r, p, q written: eight vector sweeps, against twelve for the apply and the
+// two vector kernels of the unfused iteration.
+// ---------------------------------------------------------------------------
+template <int P>
+struct CgParams {
+  double Me[EO<P>::UE], Mo[EO<P>::UO];
+  double Ke[EO<P>::UE], Ko[EO<P>::UO];
+  double rz, rx, cy;
+  double Kd[P + 1], Md[P + 1], c[3];  // 1D element diagonals and metric: the D^-1 table
+  int jacobi;
+  const double* r_in;
+  const double* q_in;
+  const double* p_in;
+  double* r_out;
+  double* q_out;
+  double* p_out;
+  double* x;
+  const double* ab;    // alpha, beta
+  const double* done;  // the pass does nothing once *done >= 2
+  double* partials;    // kCgSums per tile
+  int nfx, nfy, nfz;
+  int ntx, nty;
+};
+
+// FP64 sums of NV values over the CTA, valid in thread 0 (warps added in a fixed order).
+template <int NT, int NV>
+__device__ __forceinline__ void cta_sums(double (&v)[NV]) {
+  __shared__ double red[NV][NT / 32];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double t = v[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < NT / 32; ++w) t += red[k][w];
+      v[k] = t;
+    }
+  }
+}
+
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, bool PAIR, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+k_cartesian_cg(const __grid_constant__ CgParams<P> Q) {
+  using T = double;
+  using G = Tile<P, EX, EY, EZ, T>;
+  if (*Q.done >= 2.0) return;  // the same value in every thread
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* T1 = reinterpret_cast<T*>(smem_raw);
+  T* T2 = T1 + G::TS;
+  __shared__ double dtab[P * P * P];  // [lz][ly][lx], l = grid index mod p
+  for (int i = threadIdx.x; i < P * P * P; i += NT) {
+    const int lx = i % P, ly = (i / P) % P, lz = i / (P * P);
+    auto d1 = [&](const double* D, int l) { return l == 0 ? D[0] + D[P] : D[l]; };
+    const double d = Q.c[0] * d1(Q.Kd, lx) * d1(Q.Md, ly) * d1(Q.Md, lz) +
+                     Q.c[1] * d1(Q.Md, lx) * d1(Q.Kd, ly) * d1(Q.Md, lz) +
+                     Q.c[2] * d1(Q.Md, lx) * d1(Q.Md, ly) * d1(Q.Kd, lz);
+    dtab[i] = Q.jacobi ? 1.0 / d : 1.0;
+  }
+  EOMat<P, T> Mm, Km;
+  Mm.load(Q.Me, Q.Mo);
+  Km.load(Q.Ke, Q.Ko);
+  const T alpha = Q.ab[0], beta = Q.ab[1];
+  const int tile = (int)blockIdx.x;
+  const int tx = tile % Q.ntx, ty = (tile / Q.ntx) % Q.nty, tz = tile / (Q.ntx * Q.nty);
+  const int nfx = Q.nfx, nfy = Q.nfy, nfz = Q.nfz;
+  const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
+  const long long pz = (long long)nfx * nfy;
+  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= 0 && fx0 + G::BX <= nfx &&
+                        fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
+  __syncthreads();  // dtab
+
+  auto load_col = [&](int l, T (&c)[G::BZ]) {
+    const int x = l % G::BX, y = l / G::BX;
+    const int fx = fx0 + x, fy = fy0 + y;
+    const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
+    // owned points: box coordinates 1 .. O along each axis, inside the grid
+    const bool own = x >= 1 && x <= G::OX && y >= 1 && y <= G::OY && inxy;
+    const long long col = (long long)fx + (long long)nfx * fy;
+    const double* dcol = dtab + (y % P) * P + (x % P);
+#pragma unroll
+    for (int z = 0; z < G::BZ; ++z) {  // zero inputs (outside the grid) give zero
+      const int fz = fz0 + z;
+      const bool in = interior || (inxy && (unsigned)fz < (unsigned)nfz);
+      const long long i = col + fz * pz;
+      T r = T(0), q = T(0), pp = T(0);
+      if (in) {
+        r = __ldg(Q.r_in + i);
+        q = __ldg(Q.q_in + i);
+        pp = __ldg(Q.p_in + i);
+      }
+      const T rn = fma(-alpha, q, r);
+      c[z] = fma(beta, pp, dcol[(z % P) * P * P] * rn);
+      if (z >= 1 && z <= G::OZ && own && (interior || fz < nfz)) {
+        Q.r_out[i] = rn;
+        Q.p_out[i] = c[z];
+      }
+    }
+  };
+  tile_passes<P, EX, EY, EZ, NT, ISO, PAIR, T>(T1, T2, Mm, Km, Q.rz, Q.rx, Q.cy, load_col);
+
+  // ---- owned points: store q_k, update x, and the sums. p_k and r_k were
+  // written by this CTA before the barriers of the passes, so plain loads see
+  // them ----
+  const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
+  const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz;
+  const long long base = (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
+  constexpr int NOUT = G::OX * G::OY * G::OZ;
+  constexpr int PER = (NOUT + NT - 1) / NT;
+  auto point = [&](int k, long long& o, int& t1, int& d) {  // false outside the grid
+    const int i = threadIdx.x + k * NT;
+    const int xo = i % G::OX, r = i / G::OX, yo = r % G::OY, zo = r / G::OY;
+    o = base + xo + (long long)nfx * (yo + (long long)nfy * zo);
+    t1 = zo * G::PLANE + yo * G::RX + xo;
+    d = ((zo + 1) % P) * P * P + ((yo + 1) % P) * P + (xo + 1) % P;
+    return i < NOUT && (full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz));
+  };
+  double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // pq, rz, rr, rq, qq
+  constexpr int CH = PER < 4 ? PER : 4;  // points whose loads are in flight together
+#pragma unroll
+  for (int k0 = 0; k0 < PER; k0 += CH) {
+    T pk[CH], rk[CH], pold[CH], xv[CH];
+#pragma unroll
+    for (int j = 0; j < CH; ++j) {
+      long long o;
+      int t1, d;
+      const bool ok = k0 + j < PER && point(k0 + j, o, t1, d);
+      pk[j] = ok ? Q.p_out[o] : T(0);
+      rk[j] = ok ? Q.r_out[o] : T(0);
+      pold[j] = ok ? __ldg(Q.p_in + o) : T(0);
+      xv[j] = ok ? Q.x[o] : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < CH; ++j) {
+      long long o;
+      int t1, d;
+      if (k0 + j < PER && point(k0 + j, o, t1, d)) {
+        const T q = T1[t1];
+        Q.q_out[o] = q;
+        Q.x[o] = fma(alpha, pold[j], xv[j]);
+        const double dd = dtab[d];
+        const double zr = dd * rk[j], dq = dd * q;
+        sum[0] = fma(pk[j], q, sum[0]);
+        sum[1] = fma(rk[j], zr, sum[1]);
+        sum[2] = fma(rk[j], rk[j], sum[2]);
+        sum[3] = fma(rk[j], dq, sum[3]);
+        sum[4] = fma(q, dq, sum[4]);
+      }
+    }
+  }
+  cta_sums<NT, 5>(sum);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Q.partials[(long long)tile * kCgSums + k] = sum[k];
+  }
 }
 
 
@@ -847,6 +1048,102 @@ void run_tile2(const CartesianPlan& plan, const void* x, void* y, const CartFuse
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
+// One fused CG pass with the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
+template <int P, int EX, int EY, int EZ, int NT, bool PAIR, int MINB>
+void run_cg(const CartesianPlan& plan, const CgPass& a, cudaStream_t st) {
+  using G = Tile<P, EX, EY, EZ, double>;
+  SF_REQUIRE(!plan.slab && plan.D == 3, SF_ERR_UNSUPPORTED,
+             "the fused CG pass runs on a whole 3D mesh only");
+  CgParams<P> Q{};
+  fill_eo<P, double>(plan.M, 1.0, Q.Me, Q.Mo);
+  fill_eo<P, double>(plan.K, 1.0, Q.Ke, Q.Ko);
+  const double cx = plan.c[0], cy = plan.c[1], cz = plan.c[2];
+  Q.rz = cz / cy;
+  Q.rx = cx / cy;
+  Q.cy = cy;
+  const bool iso = (cx == cy) && (cz == cy);
+  for (int l = 0; l <= P; ++l) {
+    Q.Kd[l] = plan.K[l * (P + 1) + l];
+    Q.Md[l] = plan.M[l * (P + 1) + l];
+  }
+  for (int k = 0; k < 3; ++k) Q.c[k] = plan.c[k];
+  Q.jacobi = a.jacobi ? 1 : 0;
+  Q.r_in = a.r_in;
+  Q.q_in = a.q_in;
+  Q.p_in = a.p_in;
+  Q.r_out = a.r_out;
+  Q.q_out = a.q_out;
+  Q.p_out = a.p_out;
+  Q.x = a.x;
+  Q.ab = a.ab;
+  Q.done = a.done;
+  Q.partials = a.partials;
+  Q.nfx = plan.nx * P - 1;
+  Q.nfy = plan.ny * P - 1;
+  Q.nfz = plan.nz * P - 1;
+  Q.ntx = (plan.nx + EX - 1) / EX;
+  Q.nty = (plan.ny + EY - 1) / EY;
+  const long long tiles = (long long)Q.ntx * Q.nty * ((plan.nz + EZ - 1) / EZ);
+  SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
+  if (tiles == 0) return;
+  const size_t smem = (size_t)G::WORDS * sizeof(double);
+  auto kern = iso ? k_cartesian_cg<P, EX, EY, EZ, NT, true, PAIR, MINB>
+                  : k_cartesian_cg<P, EX, EY, EZ, NT, false, PAIR, MINB>;
+  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+struct CgCandidate {
+  void (*run)(const CartesianPlan&, const CgPass&, cudaStream_t);
+  int ex, ey, ez;
+  const char* name;
+};
+#define SF_CGT(P_, EX_, EY_, EZ_, NT_, PAIR_, MINB_)                                        \
+  {&run_cg<P_, EX_, EY_, EZ_, NT_, PAIR_, MINB_>, EX_, EY_, EZ_,                            \
+   "cg pass " #EX_ "x" #EY_ "x" #EZ_ " cells, " #NT_ " thr, " #MINB_ "/SM" ", pair " #PAIR_}
+template <int P>
+struct CgCands;
+#define SF_CGC(P_, ...) \
+  template <> struct CgCands<P_> { static constexpr CgCandidate c[] = {__VA_ARGS__}; };
+SF_CGC(1, SF_CGT(1, 8, 8, 4, 256, false, 2), SF_CGT(1, 16, 16, 8, 256, false, 2))
+SF_CGC(2, SF_CGT(2, 4, 4, 4, 256, false, 2), SF_CGT(2, 8, 4, 2, 256, false, 2),
+       SF_CGT(2, 8, 8, 4, 256, false, 2))
+SF_CGC(3, SF_CGT(3, 4, 4, 2, 256, false, 2), SF_CGT(3, 4, 4, 3, 256, false, 2),
+       SF_CGT(3, 4, 6, 4, 256, false, 2))
+SF_CGC(4, SF_CGT(4, 4, 4, 2, 256, false, 2), SF_CGT(4, 4, 4, 2, 256, true, 2),
+       SF_CGT(4, 4, 4, 2, 256, false, 3), SF_CGT(4, 4, 4, 3, 256, false, 2),
+       SF_CGT(4, 4, 4, 4, 256, false, 2), SF_CGT(4, 8, 4, 2, 256, false, 2))
+SF_CGC(5, SF_CGT(5, 2, 2, 2, 256, false, 2), SF_CGT(5, 2, 3, 3, 256, false, 2))
+SF_CGC(6, SF_CGT(6, 2, 2, 2, 256, false, 1), SF_CGT(6, 2, 3, 2, 256, false, 2))
+SF_CGC(7, SF_CGT(7, 2, 2, 1, 256, false, 1))
+SF_CGC(8, SF_CGT(8, 2, 2, 1, 256, false, 1))
+#undef SF_CGC
+#undef SF_CGT
+
+template <int P>
+int cg_cand_count() { return (int)(sizeof(CgCands<P>::c) / sizeof(CgCandidate)); }
+
+int cg_candidates_for(int SB) {
+  switch (SB - 1) {
+#define SF_CASE(P_) \
+  case P_: return cg_cand_count<P_>();
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+    default: return 0;
+  }
+}
+
+const CgCandidate& cg_candidate(int SB, int k) {
+  switch (SB - 1) {
+#define SF_CASE(P_) \
+  case P_: return CgCands<P_>::c[k >= 0 && k < cg_cand_count<P_>() ? k : 0];
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+    default: throw Error(SF_ERR_UNSUPPORTED, "no fused CG pass for this order");
+  }
+}
+
 using RunFn = void (*)(const CartesianPlan&, const void*, void*, const CartFuse&, cudaStream_t);
 using BatchFn = void (*)(const CartesianPlan&, const void*, int, long long, unsigned long long*,
                          bool, cudaStream_t);
@@ -1116,6 +1413,31 @@ long long cartesian_tiles(const CartesianPlan& plan, int dtype) {
   const Candidate& c = pick(plan, dtype, plan.choice[dtype_slot(dtype)]);
   return (long long)((plan.nx + c.ex - 1) / c.ex) * ((plan.ny + c.ey - 1) / c.ey) *
          ((plan.nz + c.ez - 1) / c.ez);
+}
+
+bool cartesian_cg_supported(const CartesianPlan& plan) {
+  return plan.ready && plan.D == 3 && !plan.slab && cg_candidates_for(plan.SB) > 0;
+}
+
+int cartesian_cg_candidates(const CartesianPlan& plan) {
+  return cartesian_cg_supported(plan) ? cg_candidates_for(plan.SB) : 0;
+}
+
+const char* cartesian_cg_candidate_name(const CartesianPlan& plan, int k) {
+  SF_REQUIRE(cartesian_cg_supported(plan), SF_ERR_UNSUPPORTED, "no fused CG pass for this operator");
+  return cg_candidate(plan.SB, k < 0 ? plan.cg_choice : k).name;
+}
+
+long long cartesian_cg_tiles(const CartesianPlan& plan, int k) {
+  SF_REQUIRE(cartesian_cg_supported(plan), SF_ERR_UNSUPPORTED, "no fused CG pass for this operator");
+  const CgCandidate& c = cg_candidate(plan.SB, k < 0 ? plan.cg_choice : k);
+  return (long long)((plan.nx + c.ex - 1) / c.ex) * ((plan.ny + c.ey - 1) / c.ey) *
+         ((plan.nz + c.ez - 1) / c.ez);
+}
+
+void cartesian_cg_pass(const CartesianPlan& plan, int k, const CgPass& a, cudaStream_t stream) {
+  SF_REQUIRE(cartesian_cg_supported(plan), SF_ERR_UNSUPPORTED, "no fused CG pass for this operator");
+  cg_candidate(plan.SB, k < 0 ? plan.cg_choice : k).run(plan, a, stream);
 }
 
 void cartesian_release(CartesianPlan& plan) { plan.ready = false; }

@@ -20,6 +20,8 @@ enum CgSlot {
   CG_PART_PQ = 10,  // distributed CG: this rank's (p, q), then (after the caller's sum) all ranks'
   CG_PART_RZ = 11,  // distributed CG: (r, dinv r), likewise
   CG_PART_RR = 12,  // distributed CG: (r, r), likewise
+  CG_ALPHA = 13,    // fused CG: alpha and beta of the last finished pass (0 before the first)
+  CG_BETA = 14,
   CG_NSLOTS = 16
 };
 
@@ -66,6 +68,13 @@ void cg_direction(double* s, T* x, T* p, const T* r, const T* dinv, long long n,
                   cudaStream_t st);
 template <typename T>
 void vec_invert(const double* d, T* dinv, long long n, cudaStream_t st);
+// After a fused CG pass (cartesian_cg_pass) over ntiles tiles: adds the passes' per-tile
+// sums in a fixed order; RR = (r_k, r_k), RZ, PQ; unless the first pass, ITERS += 1;
+// DONE = 2 once RR <= TOL2 (3 if not finite), else ALPHA = RZ / PQ and BETA from the
+// one-step recurrence for (r_{k+1}, D^-1 r_{k+1}); REPORTS += 1 and a report. Once
+// DONE >= 2 it only reports.
+void cg_fused_finish(double* s, const double* partials, long long ntiles, bool first,
+                     double* report, cudaStream_t st);
 // Reliable update: r32 = float(b - q), xs32 = 0, optionally p32 = dinv r32;
 // writes s[CG_RZ_NEW] = (r32, dinv r32) and s[CG_RR] = FP64 (r, r).
 void mixed_residual(const double* b, const double* q, const float* dinv, float* r32, float* xs32,

@@ -247,6 +247,11 @@ class LazyMatrix:
         dtype = dtype or torch.float64
         return lib.sf_kernel_name(self._h, _dtype_code(dtype)).decode()
 
+    def cg_kernel_name(self) -> str:
+        """The iteration cg() runs in its FP64 modes: the fused CG kernel's tile
+        shape, or the unfused apply + vector kernels."""
+        return lib.sf_cg_kernel_name(self._h).decode()
+
     def uses_tiled_kernel(self) -> bool:
         return self.info("tiled_kernel") == 1.0
 
