@@ -39,8 +39,9 @@ def test_fused_cg_matches_oracle(sf, p, n, mode):
     bd = torch.from_numpy(b).cuda()
     x, info = sf.cg(A, bd, reltol=1e-10, mode=mode, maxiter=20000)
     assert info["converged"] and info["relres"] <= 1e-10
-    # high orders are ill-conditioned: rounding may move the count by a little more
-    assert abs(info["iters"] - it_ref) <= max(1, it_ref // 50)
+    # equispaced high orders are ill-conditioned (Q8 Jacobi: about 1600 iterations on
+    # 2^3 cells), and rounding then moves the count by a few percent
+    assert abs(info["iters"] - it_ref) <= (1 if p <= 4 else max(10, it_ref // 10))
     assert np.abs(x.cpu().numpy() - x_ref).max() < 1e-8 * np.abs(x_ref).max()
     # the reported residual is that of the returned x
     assert true_relres(A, bd, x) < 2e-10
