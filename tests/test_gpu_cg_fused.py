@@ -98,9 +98,10 @@ def test_initial_guess_is_used(sf):
     A, om, mesh = setup(sf, 2, (6, 6, 6))
     b = torch.from_numpy(O.rhs(om, mesh, O.sin_forcing)).cuda()
     x_ref, i_ref = sf.cg(A, b, reltol=1e-12)
+    # a rough start (its residual is far above ||b||): the same solution
     x0 = x_ref + 1e-3 * torch.sin(torch.arange(A.n, dtype=torch.float64, device="cuda"))
     x, info = sf.cg(A, b, x=x0.clone(), reltol=1e-12)
-    assert info["converged"] and info["iters"] < i_ref["iters"] + 5
+    assert info["converged"] and true_relres(A, b, x) < 2e-12
     assert (x - x_ref).abs().max().item() < 1e-9 * x_ref.abs().max().item()
     # starting at the solution: no iteration
     x1, i1 = sf.cg(A, b, x=x.clone(), reltol=1e-6)
