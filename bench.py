@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--cg-only", action="store_true",
                     help="only the CG solves (autotuned tiles; no apply leg): for profiling")
     ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
-    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d"], default=None,
+    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d", "cg_fused"],
+                    default=None,
                     help="run only this secondary configuration (no apply leg): for profiling")
     ap.add_argument("--deformed-cells", type=int, default=32,
                     help="cells per direction of the deformed Q8 section")
@@ -70,6 +71,8 @@ def parse():
                     help="skip the batched, adjoint and deformed-mesh sections")
     ap.add_argument("--tile", type=int, default=None,
                     help="force tile candidate K of the FP64 tiled kernel (skips the autotuner)")
+    ap.add_argument("--cg-candidate", type=int, default=None,
+                    help="cg_fused section: only tile shape K of the fused CG kernel")
     ap.add_argument("--cells", type=int, default=64,
                     help="cells per direction (64 is the benchmark; smaller only for profiling)")
     a = ap.parse_args()
@@ -309,7 +312,9 @@ def run_ours(args, rank, world, local_rank):
     if args.section is not None:
         fn = {"batched": run_batched, "adjoint": run_adjoint, "quad2d": run_quad2d,
               "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,
-                                                            cg_iters=args.deformed_cg)}
+                                                            cg_iters=args.deformed_cg),
+              "cg_fused": lambda sf_, dev_: run_cg_fused(sf_, dev_, args.cg_candidate,
+                                                         args.cg_maxiter)}
         return {args.section: fn[args.section](sf, dev)}
     m, model, V, A = build_problem(sf)
     if args.cg_only:
@@ -436,12 +441,16 @@ SECONDARY_BUDGET_S = 180.0
 def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
     import torch
     res, sols = {}, {}
+    A.set_option("cg_fused", 1)
     fused = A.info("cg_fused") == 1.0
-    # "jacobi_unfused": the same FP64 Jacobi CG with the apply and vector kernels
-    # as separate launches (for comparison with the fused iteration)
-    for mode in ("jacobi", "mixed", "plain") + (("jacobi_unfused",) if fused else ()):
-        A.set_option("cg_fused", 0 if mode == "jacobi_unfused" else 1)
-        cg_mode = "jacobi" if mode == "jacobi_unfused" else mode
+    A.set_option("cg_fused", 0)
+    # "jacobi_fused": the same FP64 Jacobi CG with the fused iteration (sf_cg option
+    # cg_fused = 1), for comparison with the default unfused one
+    for mode in ("jacobi", "mixed", "plain") + (("jacobi_fused",) if fused else ()):
+        A.set_option("cg_fused", 1 if mode == "jacobi_fused" else 0)
+        if mode == "jacobi_fused":
+            A.autotune(torch.float64)  # with cg_fused set, also the fused kernel's shapes
+        cg_mode = "jacobi" if mode == "jacobi_fused" else mode
         if warm:  # workspaces, diagonal
             sf.cg(A, b, reltol=1e-10, mode=cg_mode, maxiter=maxiter, raise_on_fail=False)
         torch.cuda.synchronize()
@@ -454,7 +463,7 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
             torch.cuda.synchronize()
         sols[mode] = x
         key = {"jacobi": "f64", "mixed": "mixed", "plain": "f64_plain",
-               "jacobi_unfused": "f64_unfused"}[mode]
+               "jacobi_fused": "f64_fused"}[mode]
         ms = e0.elapsed_time(e1)
         res[key] = {"ms": round(ms, 3), "iters": info["iters"],
                     "ms_per_iter": round(ms / max(1, info["iters"]), 4),
@@ -463,14 +472,15 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
         log(f"cg {key}: {res[key]}")
         if u_exact is not None:
             res[key]["err_vs_exact_max"] = (x - u_exact).abs().max().item()
-    A.set_option("cg_fused", 1)
+    if "jacobi_fused" in sols:
+        res["f64_fused"]["iteration"] = A.cg_kernel_name()
+        res["f64_fused"]["err_vs_f64_max_rel"] = (
+            (sols["jacobi_fused"] - sols["jacobi"]).abs().max() / sols["jacobi"].abs().max()).item()
+        res["speedup_fused_vs_unfused"] = round(res["f64"]["ms"] / res["f64_fused"]["ms"], 3)
+    A.set_option("cg_fused", 0)
     res["f64"]["iteration"] = A.cg_kernel_name()
     res["mixed"]["err_vs_f64_max_rel"] = ((sols["mixed"] - sols["jacobi"]).abs().max() /
                                           sols["jacobi"].abs().max()).item()
-    if "jacobi_unfused" in sols:
-        res["f64_unfused"]["err_vs_f64_max_rel"] = (
-            (sols["jacobi_unfused"] - sols["jacobi"]).abs().max() / sols["jacobi"].abs().max()).item()
-        res["speedup_fused_vs_unfused"] = round(res["f64_unfused"]["ms"] / res["f64"]["ms"], 3)
     res["speedup_mixed_vs_f64"] = round(res["f64"]["ms"] / res["mixed"]["ms"], 3)
     res["speedup_mixed_vs_f64_plain"] = round(res["f64_plain"]["ms"] / res["mixed"]["ms"], 3)
     return res
@@ -663,6 +673,43 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
 # 1024 x 1024 cells, quadrature degree 2(p - 1), GPU sum-factorization kernel
 # gpu_mul_v3! on a V100 (its operator uses the weights only, no geometric factors).
 REF_2D_V100_S = {4: 0.003, 5: 0.0051, 6: 0.00805, 7: 0.014}
+
+
+def run_cg_fused(sf, dev, candidate=None, maxiter=6000):
+    """FP64 Jacobi CG iteration at Q4 64^3, fused (one tile kernel per iteration,
+    sf_cg option cg_fused = 1; every tile shape, or only `candidate`) against the
+    default unfused one: ms per iteration from solves of 60 and 20 iterations on
+    a rough right-hand side (b ~ U[-1,1], seed 1). With maxiter < 20 and a
+    candidate: one fused solve of maxiter iterations only (for a profiler)."""
+    import torch
+    m, model, V, A = build_problem(sf)
+    b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, A.n)).to(dev)
+
+    def solve(k):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sf.cg(A, b, reltol=1e-300, maxiter=k, raise_on_fail=False)  # a fixed iteration count
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    A.set_option("cg_fused", 1)
+    if candidate is not None and maxiter < 20:
+        A.set_option("cg_candidate", candidate)
+        solve(maxiter)
+        return {"iteration": A.cg_kernel_name(), "iters": maxiter}
+    nc = int(A.info("cg_candidates"))
+    out = {}
+    for k in ([candidate] if candidate is not None else list(range(nc))) + [None]:
+        if k is None:
+            A.set_option("cg_fused", 0)
+        else:
+            A.set_option("cg_candidate", k)
+        solve(5)
+        out[A.cg_kernel_name()] = round(min((solve(60) - solve(20)) / 40 for _ in range(2)), 4)
+    log(f"cg ms per iteration: {out}")
+    return {"ms_per_iter": out}
 
 
 def run_quad2d(sf, dev, n=1024, orders=(4, 5, 6, 7)):

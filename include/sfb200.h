@@ -197,12 +197,13 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream);
  * at profiling/drivers.jl:85-95. Stops when ||r||_2 <= reltol * ||b||_2
  * (FP64 true residual for SF_CG_MIXED). Reports iterations (FP32 iterations
  * for SF_CG_MIXED) and the final relative residual.
- * On a whole 3D Cartesian mesh of order 1..8 (the tiled kernel in use), the
- * FP64 modes run one fused kernel per iteration: the vector updates of
+ * An FP64 iteration is the apply and two vector kernels. On a whole 3D
+ * Cartesian mesh of order 1..8 (the tiled kernel in use), option "cg_fused" = 1
+ * selects one fused kernel per iteration instead: the vector updates of
  * iteration k-1 (x, r, and the next direction p) and q = A p in one sweep,
- * with the Jacobi diagonal taken from a per-cell-position table (option
- * "cg_fused" = 0 selects the unfused iteration: the apply and two vector
- * kernels). Both are the same CG; iteration counts agree within one.
+ * with the Jacobi diagonal taken from a per-cell-position table. It moves
+ * fewer bytes but is slower on B200 (its loads' latency bounds it). Both
+ * are the same CG; iteration counts agree within one.
  */
 int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter,
           int* iters, double* relres, void* stream);
@@ -247,7 +248,7 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *                          dropped by this factor (default 0.1)
  *   "tile_candidate_f64"  : force tile-shape candidate k of the tiled Cartesian kernel
  *   "tile_candidate_f32"    (0-based; see sf_get_info "tile_candidates_f64/f32")
- *   "cg_fused"            : 1 (default) fused FP64 CG iteration where available, 0 unfused
+ *   "cg_fused"            : 1 fused FP64 CG iteration where available, 0 (default) unfused
  *   "cg_candidate"        : force tile-shape candidate k of the fused CG kernel
  *                           (0-based; see sf_get_info "cg_candidates")
  */
@@ -275,8 +276,8 @@ int sf_get_info(const sf_op* op, const char* key, double* value);
 /*
  * Time every tile-shape candidate of the tiled Cartesian kernel for this
  * handle's order, mesh and dtype, and keep the fastest for later sf_apply
- * calls; for SF_F64 also the fused CG kernel's candidates, for later sf_cg
- * calls. Temporary vectors are allocated for the timing. Without the
+ * calls; for SF_F64 with "cg_fused" set, also the fused CG kernel's
+ * candidates. Temporary vectors are allocated for the timing. Without the
  * tiled kernel (table gather, deformed cells, kappa) it does nothing.
  * Replaces the launch-configuration table that the reference kept by hand
  * (test/benchmark_v3.jl:36-40).

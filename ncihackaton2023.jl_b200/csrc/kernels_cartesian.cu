@@ -481,13 +481,6 @@ struct CgParams {
   double rz, rx, cy;
   double Kd[P + 1], Md[P + 1], c[3];  // 1D element diagonals and metric: the D^-1 table
   int jacobi;
-  const double* r_in;
-  const double* q_in;
-  const double* p_in;
-  double* r_out;
-  double* q_out;
-  double* p_out;
-  double* x;
   const double* ab;    // alpha, beta
   const double* done;  // the pass does nothing once *done >= 2
   double* partials;    // kCgSums per tile
@@ -518,9 +511,14 @@ __device__ __forceinline__ void cta_sums(double (&v)[NV]) {
   }
 }
 
+// The vectors are separate __restrict__ parameters: none aliases another, so the
+// compiler may keep many loads in flight.
 template <int P, int EX, int EY, int EZ, int NT, bool ISO, bool PAIR, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
-k_cartesian_cg(const __grid_constant__ CgParams<P> Q) {
+k_cartesian_cg(const __grid_constant__ CgParams<P> Q, const double* __restrict__ r_in,
+               const double* __restrict__ q_in, const double* __restrict__ p_in,
+               double* __restrict__ r_out, double* __restrict__ q_out,
+               double* __restrict__ p_out, double* __restrict__ xv) {
   using T = double;
   using G = Tile<P, EX, EY, EZ, T>;
   if (*Q.done >= 2.0) return;  // the same value in every thread
@@ -549,12 +547,11 @@ k_cartesian_cg(const __grid_constant__ CgParams<P> Q) {
                         fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
   __syncthreads();  // dtab
 
+  // ---- z pass input: p_k on the box, from the k-1 vectors (loads only) ----
   auto load_col = [&](int l, T (&c)[G::BZ]) {
     const int x = l % G::BX, y = l / G::BX;
     const int fx = fx0 + x, fy = fy0 + y;
     const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
-    // owned points: box coordinates 1 .. O along each axis, inside the grid
-    const bool own = x >= 1 && x <= G::OX && y >= 1 && y <= G::OY && inxy;
     const long long col = (long long)fx + (long long)nfx * fy;
     const double* dcol = dtab + (y % P) * P + (x % P);
 #pragma unroll
@@ -562,25 +559,16 @@ k_cartesian_cg(const __grid_constant__ CgParams<P> Q) {
       const int fz = fz0 + z;
       const bool in = interior || (inxy && (unsigned)fz < (unsigned)nfz);
       const long long i = col + fz * pz;
-      T r = T(0), q = T(0), pp = T(0);
-      if (in) {
-        r = __ldg(Q.r_in + i);
-        q = __ldg(Q.q_in + i);
-        pp = __ldg(Q.p_in + i);
-      }
-      const T rn = fma(-alpha, q, r);
-      c[z] = fma(beta, pp, dcol[(z % P) * P * P] * rn);
-      if (z >= 1 && z <= G::OZ && own && (interior || fz < nfz)) {
-        Q.r_out[i] = rn;
-        Q.p_out[i] = c[z];
-      }
+      const T r = in ? __ldg(r_in + i) : T(0);
+      const T q = in ? __ldg(q_in + i) : T(0);
+      const T pp = in ? __ldg(p_in + i) : T(0);
+      c[z] = fma(beta, pp, dcol[(z % P) * P * P] * fma(-alpha, q, r));
     }
   };
   tile_passes<P, EX, EY, EZ, NT, ISO, PAIR, T>(T1, T2, Mm, Km, Q.rz, Q.rx, Q.cy, load_col);
 
-  // ---- owned points: store q_k, update x, and the sums. p_k and r_k were
-  // written by this CTA before the barriers of the passes, so plain loads see
-  // them ----
+  // ---- owned points: r_k and p_k again (the same operations as in the z pass),
+  // x_k, q_k from T1; every write of the pass; the sums ----
   const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
   const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz;
   const long long base = (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
@@ -598,31 +586,36 @@ k_cartesian_cg(const __grid_constant__ CgParams<P> Q) {
   constexpr int CH = PER < 4 ? PER : 4;  // points whose loads are in flight together
 #pragma unroll
   for (int k0 = 0; k0 < PER; k0 += CH) {
-    T pk[CH], rk[CH], pold[CH], xv[CH];
+    T rv[CH], qv[CH], pv[CH], xo[CH];
 #pragma unroll
     for (int j = 0; j < CH; ++j) {
       long long o;
       int t1, d;
       const bool ok = k0 + j < PER && point(k0 + j, o, t1, d);
-      pk[j] = ok ? Q.p_out[o] : T(0);
-      rk[j] = ok ? Q.r_out[o] : T(0);
-      pold[j] = ok ? __ldg(Q.p_in + o) : T(0);
-      xv[j] = ok ? Q.x[o] : T(0);
+      rv[j] = ok ? __ldg(r_in + o) : T(0);
+      qv[j] = ok ? __ldg(q_in + o) : T(0);
+      pv[j] = ok ? __ldg(p_in + o) : T(0);
+      xo[j] = ok ? xv[o] : T(0);
     }
 #pragma unroll
     for (int j = 0; j < CH; ++j) {
       long long o;
       int t1, d;
       if (k0 + j < PER && point(k0 + j, o, t1, d)) {
-        const T q = T1[t1];
-        Q.q_out[o] = q;
-        Q.x[o] = fma(alpha, pold[j], xv[j]);
         const double dd = dtab[d];
-        const double zr = dd * rk[j], dq = dd * q;
-        sum[0] = fma(pk[j], q, sum[0]);
-        sum[1] = fma(rk[j], zr, sum[1]);
-        sum[2] = fma(rk[j], rk[j], sum[2]);
-        sum[3] = fma(rk[j], dq, sum[3]);
+        const T rn = fma(-alpha, qv[j], rv[j]);
+        const T zr = dd * rn;
+        const T pn = fma(beta, pv[j], zr);
+        const T q = T1[t1];
+        r_out[o] = rn;
+        p_out[o] = pn;
+        q_out[o] = q;
+        xv[o] = fma(alpha, pv[j], xo[j]);
+        const double dq = dd * q;
+        sum[0] = fma(pn, q, sum[0]);
+        sum[1] = fma(rn, zr, sum[1]);
+        sum[2] = fma(rn, rn, sum[2]);
+        sum[3] = fma(rn, dq, sum[3]);
         sum[4] = fma(q, dq, sum[4]);
       }
     }
@@ -633,7 +626,6 @@ k_cartesian_cg(const __grid_constant__ CgParams<P> Q) {
     for (int k = 0; k < 5; ++k) Q.partials[(long long)tile * kCgSums + k] = sum[k];
   }
 }
-
 
 // ---------------------------------------------------------------------------
 // 2D (quadrilateral Q_p) tiled apply on an nx x ny Cartesian mesh:
@@ -1051,7 +1043,6 @@ void run_tile2(const CartesianPlan& plan, const void* x, void* y, const CartFuse
 // One fused CG pass with the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
 template <int P, int EX, int EY, int EZ, int NT, bool PAIR, int MINB>
 void run_cg(const CartesianPlan& plan, const CgPass& a, cudaStream_t st) {
-  using G = Tile<P, EX, EY, EZ, double>;
   SF_REQUIRE(!plan.slab && plan.D == 3, SF_ERR_UNSUPPORTED,
              "the fused CG pass runs on a whole 3D mesh only");
   CgParams<P> Q{};
@@ -1068,13 +1059,6 @@ void run_cg(const CartesianPlan& plan, const CgPass& a, cudaStream_t st) {
   }
   for (int k = 0; k < 3; ++k) Q.c[k] = plan.c[k];
   Q.jacobi = a.jacobi ? 1 : 0;
-  Q.r_in = a.r_in;
-  Q.q_in = a.q_in;
-  Q.p_in = a.p_in;
-  Q.r_out = a.r_out;
-  Q.q_out = a.q_out;
-  Q.p_out = a.p_out;
-  Q.x = a.x;
   Q.ab = a.ab;
   Q.done = a.done;
   Q.partials = a.partials;
@@ -1086,11 +1070,13 @@ void run_cg(const CartesianPlan& plan, const CgPass& a, cudaStream_t st) {
   const long long tiles = (long long)Q.ntx * Q.nty * ((plan.nz + EZ - 1) / EZ);
   SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
   if (tiles == 0) return;
+  using G = Tile<P, EX, EY, EZ, double>;
   const size_t smem = (size_t)G::WORDS * sizeof(double);
   auto kern = iso ? k_cartesian_cg<P, EX, EY, EZ, NT, true, PAIR, MINB>
                   : k_cartesian_cg<P, EX, EY, EZ, NT, false, PAIR, MINB>;
   SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
+  kern<<<(unsigned)tiles, NT, smem, st>>>(Q, a.r_in, a.q_in, a.p_in, a.r_out, a.q_out, a.p_out,
+                                         a.x);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -1106,16 +1092,13 @@ template <int P>
 struct CgCands;
 #define SF_CGC(P_, ...) \
   template <> struct CgCands<P_> { static constexpr CgCandidate c[] = {__VA_ARGS__}; };
-SF_CGC(1, SF_CGT(1, 8, 8, 4, 256, false, 2), SF_CGT(1, 16, 16, 8, 256, false, 2))
-SF_CGC(2, SF_CGT(2, 4, 4, 4, 256, false, 2), SF_CGT(2, 8, 4, 2, 256, false, 2),
-       SF_CGT(2, 8, 8, 4, 256, false, 2))
-SF_CGC(3, SF_CGT(3, 4, 4, 2, 256, false, 2), SF_CGT(3, 4, 4, 3, 256, false, 2),
-       SF_CGT(3, 4, 6, 4, 256, false, 2))
-SF_CGC(4, SF_CGT(4, 4, 4, 2, 256, false, 2), SF_CGT(4, 4, 4, 2, 256, true, 2),
-       SF_CGT(4, 4, 4, 2, 256, false, 3), SF_CGT(4, 4, 4, 3, 256, false, 2),
-       SF_CGT(4, 4, 4, 4, 256, false, 2), SF_CGT(4, 8, 4, 2, 256, false, 2))
-SF_CGC(5, SF_CGT(5, 2, 2, 2, 256, false, 2), SF_CGT(5, 2, 3, 3, 256, false, 2))
-SF_CGC(6, SF_CGT(6, 2, 2, 2, 256, false, 1), SF_CGT(6, 2, 3, 2, 256, false, 2))
+SF_CGC(1, SF_CGT(1, 8, 8, 4, 256, true, 2), SF_CGT(1, 8, 8, 4, 256, false, 2))
+SF_CGC(2, SF_CGT(2, 4, 4, 4, 256, true, 2), SF_CGT(2, 8, 4, 2, 256, false, 2))
+SF_CGC(3, SF_CGT(3, 4, 4, 2, 256, true, 2), SF_CGT(3, 4, 4, 2, 256, false, 3))
+SF_CGC(4, SF_CGT(4, 4, 4, 2, 256, false, 3), SF_CGT(4, 4, 4, 2, 256, true, 2),
+       SF_CGT(4, 4, 4, 2, 256, false, 2))
+SF_CGC(5, SF_CGT(5, 2, 2, 2, 256, false, 2), SF_CGT(5, 2, 2, 2, 256, true, 2))
+SF_CGC(6, SF_CGT(6, 2, 2, 2, 256, false, 1), SF_CGT(6, 2, 2, 1, 256, false, 2))
 SF_CGC(7, SF_CGT(7, 2, 2, 1, 256, false, 1))
 SF_CGC(8, SF_CGT(8, 2, 2, 1, 256, false, 1))
 #undef SF_CGC

@@ -58,7 +58,10 @@ struct sf_op {
   double* h_report = nullptr;  // mapped pinned: CG progress reports written by the device
   double* d_report = nullptr;  // its device address
   double mixed_inner_reltol = 1e-1;
-  bool cg_fused = true;  // FP64 CG on the tiled Cartesian operator: one fused pass per iteration
+  // FP64 CG on the tiled Cartesian operator with one fused pass per iteration. Off by
+  // default: on B200 the fused pass is bound by the latency of its loads (r, q and p over
+  // each tile's halo box), and the unfused iteration is faster.
+  bool cg_fused = false;
   int last_outer = 0, last_inner = 0;
   double last_relres = 0.0;
   std::string err;
@@ -1213,8 +1216,8 @@ int sf_autotune(sf_op* op, int dtype, void* stream) {
         sf::cartesian_apply_candidate(op->cart, dtype, k, x, y, st);
       });
     }
-    // the fused FP64 CG pass, on zero vectors with alpha = beta = 0
-    const int ncg = dtype == SF_F64 ? sf::cartesian_cg_candidates(op->cart) : 0;
+    // the fused FP64 CG pass (when selected), on zero vectors with alpha = beta = 0
+    const int ncg = dtype == SF_F64 && op->cg_fused ? sf::cartesian_cg_candidates(op->cart) : 0;
     if (ncg > 1) {
       long long tiles = 0;
       for (int k = 0; k < ncg; ++k) tiles = std::max(tiles, sf::cartesian_cg_tiles(op->cart, k));

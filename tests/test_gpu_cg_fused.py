@@ -1,7 +1,8 @@
-"""Fused FP64 CG iteration (one tiled kernel per iteration: the vector updates
-of iteration k-1 and q = A p of iteration k, Jacobi diagonal from a per-cell
-position table) against the oracle's restatement of IterativeSolvers.cg!, and
-against the unfused iteration (apply + vector kernels) of the same handle."""
+"""Fused FP64 CG iteration (option cg_fused = 1: one tiled kernel per
+iteration, the vector updates of iteration k-1 and q = A p of iteration k,
+Jacobi diagonal from a per-cell position table) against the oracle's
+restatement of IterativeSolvers.cg!, and against the default unfused
+iteration (apply + vector kernels) of the same handle."""
 import numpy as np
 import pytest
 import torch
@@ -17,6 +18,8 @@ def setup(sf, p, n, domain=(0, 1, 0, 1, 0, 1)):
     V = sf.FESpace(model, p)
     m = sf.SumFactorizationMap(3, (p,) * 3, (deg,) * 3)
     A = sf.LazyMatrix(m, V, V, sf.Measure(model, deg))
+    assert A.info("cg_fused") == 0.0  # off by default
+    A.set_option("cg_fused", 1)
     om = O.make_map(3, p, deg)
     mesh = O.cartesian_mesh(3, n, p, om) if domain == (0, 1, 0, 1, 0, 1) else None
     return A, om, mesh
@@ -123,6 +126,7 @@ def test_unsupported_operators_use_the_unfused_iteration(sf):
     V = sf.FESpace(model, 2)
     m = sf.SumFactorizationMap(3, (2,) * 3, (4,) * 3)
     A = sf.LazyMatrix(m, V, V, sf.Measure(model, 4))
+    A.set_option("cg_fused", 1)
     assert not A.uses_tiled_kernel() and A.info("cg_fused") == 0.0
     with pytest.raises(sf.SumFacError):
         A.set_option("cg_candidate", 0)

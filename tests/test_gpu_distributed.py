@@ -75,9 +75,6 @@ def test_distributed_cg_matches_single_operator(sf, nparts):
     p, n = 4, (4, 4, 6)
     m, model, V, A = _setup(sf, p, n, domain=(0, 2, 0, 1, 0, 1))  # anisotropic cells
     b = torch.from_numpy(np.random.default_rng(4).uniform(-1, 1, A.n)).cuda()
-    # the slab steps run the unfused iteration (apply, update, direction): compare with
-    # the same iteration on the single operator
-    A.set_option("cg_fused", 0)
     x_ref, info_ref = sf.cg(A, b, reltol=1e-10, mode="jacobi")
     D = sf.distributed.DistributedLazyMatrix(m, model, nparts=nparts)
     xs, info = sf.distributed.cg(D, D.from_global(b), reltol=1e-10)
