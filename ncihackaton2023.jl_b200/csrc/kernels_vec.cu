@@ -325,6 +325,148 @@ __global__ void k_cg_fused_finish(double* __restrict__ s, const double* __restri
   publish(s, report);
 }
 
+// Free-grid position (x, y, z) of a flat index. A grid-stride loop advances it by the
+// position of the stride with one carry per axis, so no division per element.
+struct GridPos {
+  int x, y, z;
+  __device__ __forceinline__ void set(long long i, int nfx, int nfy) {
+    x = (int)(i % nfx);
+    const long long t = i / nfx;
+    y = (int)(t % nfy);
+    z = (int)(t / nfy);
+  }
+  __device__ __forceinline__ void add(const GridPos& d, int nfx, int nfy) {
+    x += d.x;
+    if (x >= nfx) {
+      x -= nfx;
+      ++y;
+    }
+    y += d.y;
+    if (y >= nfy) {
+      y -= nfy;
+      ++z;
+    }
+    z += d.z;
+  }
+};
+
+template <int P>
+__device__ __forceinline__ double table_dinv(const JacobiTable& J, const GridPos& g) {
+  return __ldg(J.tab + ((g.z + 1) % P) * P * P + ((g.y + 1) % P) * P + (g.x + 1) % P);
+}
+
+// k_cg_update (non-distributed) with D^-1 from the table.
+template <typename T, int P>
+__global__ void k_cg_update_table(double* __restrict__ s, T* __restrict__ r,
+                                  const T* __restrict__ q, const JacobiTable J, long long n,
+                                  double* __restrict__ partials) {
+  if (s[CG_DONE] != 0.0) return;
+  const T alpha = (T)(s[CG_RZ] / s[CG_PQ]);
+  const long long S = (long long)gridDim.x * kThreads;
+  long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+  GridPos g, st;
+  g.set(i, J.nfx, J.nfy);
+  st.set(S, J.nfx, J.nfy);
+  double v[2] = {0.0, 0.0};
+  for (; i + (kUnroll - 1) * S < n; i += kUnroll * S) {
+    T qv[kUnroll], rv[kUnroll], dv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      qv[u] = q[i + u * S];
+      rv[u] = r[i + u * S];
+      dv[u] = (T)table_dinv<P>(J, g);
+      g.add(st, J.nfx, J.nfy);
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const T ri = fma(-alpha, qv[u], rv[u]);
+      r[i + u * S] = ri;
+      const T zi = (T)(dv[u] * ri);
+      v[0] += (double)ri * (double)zi;
+      v[1] += (double)ri * (double)ri;
+    }
+  }
+  for (; i < n; i += S) {
+    const T ri = fma(-alpha, q[i], r[i]);
+    r[i] = ri;
+    const T zi = (T)((T)table_dinv<P>(J, g) * ri);
+    g.add(st, J.nfx, J.nfy);
+    v[0] += (double)ri * (double)zi;
+    v[1] += (double)ri * (double)ri;
+  }
+  if (last_block_sum<2>(v, partials, cg_counter(s)) && threadIdx.x == 0) {
+    s[CG_RZ_NEW] = v[0];
+    s[CG_RR] = v[1];
+    if (!isfinite(v[1]) || !isfinite(v[0])) s[CG_DONE] = 3.0;
+    else if (v[1] <= s[CG_TOL2]) s[CG_DONE] = 1.0;
+  }
+}
+
+// k_cg_direction with D^-1 from the table.
+template <typename T, int P>
+__global__ void k_cg_direction_table(double* __restrict__ s, T* __restrict__ x,
+                                     T* __restrict__ p, const T* __restrict__ r,
+                                     const JacobiTable J, long long n,
+                                     double* __restrict__ report) {
+  const double done = s[CG_DONE];
+  if (done >= 2.0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      s[CG_REPORTS] += 1.0;
+      publish(s, report);
+    }
+    return;
+  }
+  const T alpha = (T)(s[CG_RZ] / s[CG_PQ]);
+  const T beta = (T)(s[CG_RZ_NEW] / s[CG_RZ]);
+  const long long S = (long long)gridDim.x * kThreads;
+  long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+  if (done == 0.0) {
+    GridPos g, st;
+    g.set(i, J.nfx, J.nfy);
+    st.set(S, J.nfx, J.nfy);
+    for (; i + (kUnroll - 1) * S < n; i += kUnroll * S) {
+      T pv[kUnroll], xv[kUnroll], rv[kUnroll], dv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        pv[u] = p[i + u * S];
+        xv[u] = x[i + u * S];
+        rv[u] = r[i + u * S];
+        dv[u] = (T)table_dinv<P>(J, g);
+        g.add(st, J.nfx, J.nfy);
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        x[i + u * S] = fma(alpha, pv[u], xv[u]);
+        const T zi = (T)(dv[u] * rv[u]);
+        p[i + u * S] = fma(beta, pv[u], zi);
+      }
+    }
+    for (; i < n; i += S) {
+      const T pi = p[i];
+      x[i] = fma(alpha, pi, x[i]);
+      const T zi = (T)((T)table_dinv<P>(J, g) * r[i]);
+      g.add(st, J.nfx, J.nfy);
+      p[i] = fma(beta, pi, zi);
+    }
+  } else {
+    for (; i < n; i += S) x[i] = fma(alpha, p[i], x[i]);
+  }
+  __shared__ bool is_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    is_last = atomicAdd(cg_counter(s), 1u) == gridDim.x - 1;
+    if (is_last) {
+      *cg_counter(s) = 0u;
+      s[CG_RZ] = s[CG_RZ_NEW];
+      s[CG_ITERS] += 1.0;
+      if (done == 1.0) s[CG_DONE] = 2.0;
+      s[CG_REPORTS] += 1.0;
+      publish(s, report);
+    }
+  }
+}
+
 __global__ void k_copy_scalar(double* __restrict__ s, int dst, int src) {
   if (threadIdx.x == 0 && blockIdx.x == 0) s[dst] = s[src];
 }
@@ -474,6 +616,38 @@ void copy_scalar(double* s, int dst, int src, cudaStream_t st) {
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
+template <typename T>
+void cg_update_table(double* s, T* r, const T* q, const JacobiTable& J, long long n,
+                     double* partials, cudaStream_t st) {
+  switch (J.p) {
+#define SF_CASE(P_)                                                                            \
+  case P_:                                                                                     \
+    k_cg_update_table<T, P_><<<grid_for(k_cg_update_table<T, P_>, n), kThreads, 0, st>>>(    \
+        s, r, q, J, n, partials);                                                              \
+    break;
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+    default: throw Error(SF_ERR_UNSUPPORTED, "no Jacobi table for this order");
+  }
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+template <typename T>
+void cg_direction_table(double* s, T* x, T* p, const T* r, const JacobiTable& J, long long n,
+                        double* report, cudaStream_t st) {
+  switch (J.p) {
+#define SF_CASE(P_)                                                                            \
+  case P_:                                                                                     \
+    k_cg_direction_table<T, P_><<<grid_for(k_cg_direction_table<T, P_>, n), kThreads, 0,     \
+                                  st>>>(s, x, p, r, J, n, report);                             \
+    break;
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+    default: throw Error(SF_ERR_UNSUPPORTED, "no Jacobi table for this order");
+  }
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
 void cg_fused_finish(double* s, const double* partials, long long ntiles, bool first,
                      double* report, cudaStream_t st) {
   k_cg_fused_finish<<<1, kThreads, 0, st>>>(s, partials, ntiles, first ? 1 : 0, report);
@@ -489,7 +663,11 @@ void cg_fused_finish(double* s, const double* partials, long long ntiles, bool f
                              bool);                                                             \
   template void cg_direction<T>(double*, T*, T*, const T*, const T*, long long, double*,        \
                                 cudaStream_t);                                                  \
-  template void vec_invert<T>(const double*, T*, long long, cudaStream_t);
+  template void vec_invert<T>(const double*, T*, long long, cudaStream_t);                   \
+  template void cg_update_table<T>(double*, T*, const T*, const JacobiTable&, long long,       \
+                                   double*, cudaStream_t);                                      \
+  template void cg_direction_table<T>(double*, T*, T*, const T*, const JacobiTable&, long long, \
+                                      double*, cudaStream_t);
 SF_INST(double)
 SF_INST(float)
 #undef SF_INST

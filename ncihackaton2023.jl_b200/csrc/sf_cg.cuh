@@ -68,6 +68,23 @@ void cg_direction(double* s, T* x, T* p, const T* r, const T* dinv, long long n,
                   cudaStream_t st);
 template <typename T>
 void vec_invert(const double* d, T* dinv, long long n, cudaStream_t st);
+
+// Inverse Jacobi diagonal of a whole-mesh 3D Cartesian operator as a table: on such a
+// mesh diag(A) at a free point depends only on the point's position inside its cell,
+// so D^-1 at free point (x, y, z) (flat index x + nfx (y + nfy z)) is
+// tab[((z+1) % p) p^2 + ((y+1) % p) p + (x+1) % p], p^3 FP64 entries on the device.
+struct JacobiTable {
+  const double* tab = nullptr;
+  int p = 0, nfx = 0, nfy = 0;
+};
+// cg_update and cg_direction (non-distributed) with D^-1 from the table instead of a
+// vector: two vector sweeps fewer per iteration.
+template <typename T>
+void cg_update_table(double* s, T* r, const T* q, const JacobiTable& J, long long n,
+                     double* partials, cudaStream_t st);
+template <typename T>
+void cg_direction_table(double* s, T* x, T* p, const T* r, const JacobiTable& J, long long n,
+                        double* report, cudaStream_t st);
 // After a fused CG pass (cartesian_cg_pass) over ntiles tiles: adds the passes' per-tile
 // sums in a fixed order; RR = (r_k, r_k), RZ, PQ; unless the first pass, ITERS += 1;
 // DONE = 2 once RR <= TOL2 (3 if not finite), else ALPHA = RZ / PQ and BETA from the

@@ -47,6 +47,8 @@ struct sf_op {
   double* d_dinv = nullptr;  // 1 / diag(A) on the owned points (distributed CG)
   // workspaces
   double* d_diag = nullptr;  // FP64 diag(A), cached
+  double* d_jtab = nullptr;  // inverse Jacobi diagonal per position in a cell (Cartesian), cached
+  bool jacobi_table = true;  // CG vector kernels read D^-1 from d_jtab where it exists
   void* d_ws = nullptr;
   size_t ws_bytes = 0;
   double* d_hx = nullptr;    // sf_mul_host staging
@@ -291,6 +293,8 @@ const double* ensure_dinv(sf_op* op, cudaStream_t st) {
 void invalidate_caches(sf_op* op) {
   dfree(op->d_diag);
   op->d_diag = nullptr;
+  dfree(op->d_jtab);
+  op->d_jtab = nullptr;
   dfree(op->d_dinv);
   op->d_dinv = nullptr;
 }
@@ -463,6 +467,38 @@ int cg_f64_fused(sf_op* op, bool jacobi, const double* b, double* x, double relt
   return (int)h[kIters];
 }
 
+// D^-1 of a whole-mesh 3D Cartesian operator as a p^3 table (sf::JacobiTable), or
+// p = 0 where there is none (the CG then reads a D^-1 vector). The table is the
+// Kronecker-form diagonal of cartesian_diag, inverted, per position in a cell.
+sf::JacobiTable jacobi_table(sf_op* op) {
+  sf::JacobiTable J;
+  if (!op->jacobi_table || op->slab || !tiled(op, SF_F64)) return J;
+  const int P = op->SB - 1;
+  if (!op->d_jtab) {
+    const int SB = op->SB;
+    const double* M = op->cart.M;
+    const double* K = op->cart.K;
+    auto d1 = [&](const double* D, int l) { return l == 0 ? D[0] + D[P * SB + P] : D[l * SB + l]; };
+    std::vector<double> tab((size_t)P * P * P);
+    for (int lz = 0; lz < P; ++lz)
+      for (int ly = 0; ly < P; ++ly)
+        for (int lx = 0; lx < P; ++lx) {
+          const double d = op->cart.c[0] * d1(K, lx) * d1(M, ly) * d1(M, lz) +
+                           op->cart.c[1] * d1(M, lx) * d1(K, ly) * d1(M, lz) +
+                           op->cart.c[2] * d1(M, lx) * d1(M, ly) * d1(K, lz);
+          tab[((size_t)lz * P + ly) * P + lx] = 1.0 / d;
+        }
+    op->d_jtab = dalloc<double>(tab.size());
+    SF_CUDA_CHECK(cudaMemcpy(op->d_jtab, tab.data(), tab.size() * sizeof(double),
+                             cudaMemcpyHostToDevice));
+  }
+  J.tab = op->d_jtab;
+  J.p = P;
+  J.nfx = op->cells.nx * P - 1;
+  J.nfy = op->cells.ny * P - 1;
+  return J;
+}
+
 // Plain or Jacobi FP64 CG. Returns iterations; sets relres.
 int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, int maxiter,
            double* relres, cudaStream_t st) {
@@ -483,6 +519,7 @@ int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, in
     sf::vec_invert<double>(op->d_diag, dinv, n, st);
   }
   const double* Dv = jacobi ? dinv : nullptr;
+  const sf::JacobiTable J = jacobi ? jacobi_table(op) : sf::JacobiTable{};
   sf::cg_reset(s, st);
   apply_impl(op, SF_F64, x, q, st);
   sf::cg_start<double>(b, q, Dv, r, p, n, partials, s, st);
@@ -494,8 +531,13 @@ int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, in
   reset_reports(op);
   for (int it = 0; it < maxiter && done == 0.0;) {
     apply_pq<double>(op, p, q, partials, s, st);
-    sf::cg_update<double>(s, r, q, Dv, n, partials, st);
-    sf::cg_direction<double>(s, x, p, r, Dv, n, op->d_report, st);
+    if (J.p > 0) {  // D^-1 from the table: two vector sweeps fewer
+      sf::cg_update_table<double>(s, r, q, J, n, partials, st);
+      sf::cg_direction_table<double>(s, x, p, r, J, n, op->d_report, st);
+    } else {
+      sf::cg_update<double>(s, r, q, Dv, n, partials, st);
+      sf::cg_direction<double>(s, x, p, r, Dv, n, op->d_report, st);
+    }
     ++it;
     if (it > kCgLag) done = wait_report(op, it - kCgLag, st).done;
   }
@@ -533,6 +575,7 @@ int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, 
   double* partials = reinterpret_cast<double*>(ws + v8 + 5 * v4 + sb);
   ensure_diag(op, st);
   sf::vec_invert<float>(op->d_diag, dinv32, n, st);
+  const sf::JacobiTable J = jacobi_table(op);
   sf::cg_reset(s, st);
   sf::vec_dot<double>(b, b, n, partials, s + sf::CG_BB, s, nullptr, st);
   // true residual of the initial guess; p = dinv r; the device never stops on its own
@@ -552,8 +595,13 @@ int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, 
   reset_reports(op);
   while (rr64 > tol2 && it < maxiter) {
     apply_pq<float>(op, p32, q32, partials, s, st);
-    sf::cg_update<float>(s, r32, q32, dinv32, n, partials, st);
-    sf::cg_direction<float>(s, xs32, p32, r32, dinv32, n, op->d_report, st);
+    if (J.p > 0) {
+      sf::cg_update_table<float>(s, r32, q32, J, n, partials, st);
+      sf::cg_direction_table<float>(s, xs32, p32, r32, J, n, op->d_report, st);
+    } else {
+      sf::cg_update<float>(s, r32, q32, dinv32, n, partials, st);
+      sf::cg_direction<float>(s, xs32, p32, r32, dinv32, n, op->d_report, st);
+    }
     ++it;
     dirty = true;
     bool refine = it >= maxiter;
@@ -699,6 +747,7 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_wdet);
   dfree(op->d_kappa);
   dfree(op->d_diag);
+  dfree(op->d_jtab);
   dfree(op->d_dinv);
   dfree(op->d_ws);
   dfree(op->d_hx);
@@ -1176,6 +1225,9 @@ int sf_set_option(sf_op* op, const char* name, double value) {
     if (n == "mixed_inner_reltol") {
       SF_REQUIRE(value > 0 && value < 1, SF_ERR_ARG, "mixed_inner_reltol must be in (0,1)");
       op->mixed_inner_reltol = value;
+    } else if (n == "jacobi_table") {
+      SF_REQUIRE(value == 0 || value == 1, SF_ERR_ARG, "jacobi_table must be 0 or 1");
+      op->jacobi_table = value == 1;
     } else if (n == "cg_fused") {
       SF_REQUIRE(value == 0 || value == 1, SF_ERR_ARG, "cg_fused must be 0 or 1");
       op->cg_fused = value == 1;
@@ -1270,6 +1322,8 @@ int sf_get_info(const sf_op* op, const char* key, double* value) {
   else if (k == "geometry_kind") *value = (double)op->geom.kind;
   else if (k == "slab") *value = op->slab ? 1.0 : 0.0;
   else if (k == "cg_fused") *value = use_fused_cg(op) ? 1.0 : 0.0;
+  else if (k == "jacobi_table")
+    *value = (op->jacobi_table && !op->slab && tiled && op->D == 3) ? 1.0 : 0.0;
   else if (k == "cg_candidates") *value = (double)sf::cartesian_cg_candidates(op->cart);
   else if (k == "plane_size") *value = (double)op->plane;
   else if (k == "owned_offset") *value = (double)owned_offset(op);

@@ -115,3 +115,25 @@ def test_cg_tiled_and_general_paths_agree(sf):
     x_g, i_g = sf.cg(Ag, bg, reltol=1e-11, mode="jacobi")
     assert abs(i_t["iters"] - i_g["iters"]) <= 1
     assert (x_g[perm] - x_t).abs().max().item() < 1e-9 * x_t.abs().max().item()
+
+
+@pytest.mark.parametrize("mode", ["jacobi", "mixed"])
+def test_jacobi_table_and_vector_agree(sf, mode):
+    """On a Cartesian mesh the CG vector kernels read D^-1 from a table per position
+    in a cell (option jacobi_table, the default); the D^-1 vector gives the same CG.
+    Anisotropic cells, several orders."""
+    import torch
+    for p, n, dom in ((3, (7, 5, 6), (0, 2, 0, 1, 0, 0.5)), (4, (5, 6, 4), (0, 1, 0, 3, 0, 1))):
+        model = sf.CartesianDiscreteModel(dom, n)
+        V = sf.FESpace(model, p)
+        m = sf.SumFactorizationMap(3, (p,) * 3, (2 * p,) * 3)
+        A = sf.LazyMatrix(m, V, V, sf.Measure(model, 2 * p))
+        assert A.info("jacobi_table") == 1.0
+        b = torch.from_numpy(np.random.default_rng(p).uniform(-1, 1, A.n)).cuda()
+        x_t, i_t = sf.cg(A, b, reltol=1e-10, mode=mode)
+        A.set_option("jacobi_table", 0)
+        assert A.info("jacobi_table") == 0.0
+        x_v, i_v = sf.cg(A, b, reltol=1e-10, mode=mode)
+        assert i_t["converged"] and i_v["converged"]
+        assert abs(i_t["iters"] - i_v["iters"]) <= (1 if mode == "jacobi" else 20)
+        assert (x_t - x_v).abs().max().item() < 1e-8 * x_v.abs().max().item()
