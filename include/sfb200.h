@@ -248,9 +248,9 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *                          dropped by this factor (default 0.1)
  *   "tile_candidate_f64"  : force tile-shape candidate k of the tiled Cartesian kernel
  *   "tile_candidate_f32"    (0-based; see sf_get_info "tile_candidates_f64/f32")
- *   "jacobi_table"        : 1 (default): on a whole 3D Cartesian mesh the CG vector kernels
- *                           read D^-1 from a table per position in a cell (it repeats
- *                           cell to cell) instead of a vector; 0: from the vector
+ *   "jacobi_table"        : 1 (default): on a whole 3D Cartesian mesh the FP64 Jacobi CG's
+ *                           vector kernels read D^-1 from a table per position in a cell
+ *                           (it repeats cell to cell) instead of a vector; 0: from the vector
  *   "cg_fused"            : 1 fused FP64 CG iteration where available, 0 (default) unfused
  *   "cg_candidate"        : force tile-shape candidate k of the fused CG kernel
  *                           (0-based; see sf_get_info "cg_candidates")
@@ -271,7 +271,7 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *   "plane_size"             : free points per z-level (structured meshes)
  *   "owned_offset", "owned_count": the points sf_apply writes (the whole vector
  *                              unless the operator is a slab)
- *   "jacobi_table"           : 1 if sf_cg's Jacobi modes read D^-1 from the table
+ *   "jacobi_table"           : 1 if sf_cg's FP64 Jacobi mode reads D^-1 from the table
  *   "cg_fused"               : 1 if sf_cg's FP64 modes use the fused CG kernel
  *   "cg_candidates"          : number of tile shapes of the fused CG kernel
  */

@@ -575,7 +575,6 @@ int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, 
   double* partials = reinterpret_cast<double*>(ws + v8 + 5 * v4 + sb);
   ensure_diag(op, st);
   sf::vec_invert<float>(op->d_diag, dinv32, n, st);
-  const sf::JacobiTable J = jacobi_table(op);
   sf::cg_reset(s, st);
   sf::vec_dot<double>(b, b, n, partials, s + sf::CG_BB, s, nullptr, st);
   // true residual of the initial guess; p = dinv r; the device never stops on its own
@@ -595,13 +594,10 @@ int cg_mixed(sf_op* op, const double* b, double* x, double reltol, int maxiter, 
   reset_reports(op);
   while (rr64 > tol2 && it < maxiter) {
     apply_pq<float>(op, p32, q32, partials, s, st);
-    if (J.p > 0) {
-      sf::cg_update_table<float>(s, r32, q32, J, n, partials, st);
-      sf::cg_direction_table<float>(s, xs32, p32, r32, J, n, op->d_report, st);
-    } else {
-      sf::cg_update<float>(s, r32, q32, dinv32, n, partials, st);
-      sf::cg_direction<float>(s, xs32, p32, r32, dinv32, n, op->d_report, st);
-    }
+    // D^-1 from the FP32 vector: at 4 bytes per element the table's index arithmetic
+    // costs more than the vector sweep it saves (measured)
+    sf::cg_update<float>(s, r32, q32, dinv32, n, partials, st);
+    sf::cg_direction<float>(s, xs32, p32, r32, dinv32, n, op->d_report, st);
     ++it;
     dirty = true;
     bool refine = it >= maxiter;

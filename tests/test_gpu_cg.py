@@ -119,9 +119,10 @@ def test_cg_tiled_and_general_paths_agree(sf):
 
 @pytest.mark.parametrize("mode", ["jacobi", "mixed"])
 def test_jacobi_table_and_vector_agree(sf, mode):
-    """On a Cartesian mesh the CG vector kernels read D^-1 from a table per position
-    in a cell (option jacobi_table, the default); the D^-1 vector gives the same CG.
-    Anisotropic cells, several orders."""
+    """On a Cartesian mesh the FP64 Jacobi CG's vector kernels read D^-1 from a table
+    per position in a cell (option jacobi_table, the default); the D^-1 vector gives
+    the same CG (the mixed mode reads the FP32 vector either way). Anisotropic
+    cells, several orders."""
     import torch
     for p, n, dom in ((3, (7, 5, 6), (0, 2, 0, 1, 0, 0.5)), (4, (5, 6, 4), (0, 1, 0, 3, 0, 1))):
         model = sf.CartesianDiscreteModel(dom, n)
