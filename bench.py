@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--cg-only", action="store_true",
                     help="only the CG solves (autotuned tiles; no apply leg): for profiling")
     ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
-    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d", "cg_fused"],
+    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d", "cg_fused",
+                                          "table_gather"],
                     default=None,
                     help="run only this secondary configuration (no apply leg): for profiling")
     ap.add_argument("--deformed-cells", type=int, default=32,
@@ -314,7 +315,8 @@ def run_ours(args, rank, world, local_rank):
               "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,
                                                             cg_iters=args.deformed_cg),
               "cg_fused": lambda sf_, dev_: run_cg_fused(sf_, dev_, args.cg_candidate,
-                                                         args.cg_maxiter)}
+                                                         args.cg_maxiter),
+              "table_gather": run_table_gather}
         return {args.section: fn[args.section](sf, dev)}
     m, model, V, A = build_problem(sf)
     if args.cg_only:
@@ -710,6 +712,38 @@ def run_cg_fused(sf, dev, candidate=None, maxiter=6000):
         out[A.cg_kernel_name()] = round(min((solve(60) - solve(20)) / 40 for _ in range(2)), 4)
     log(f"cg ms per iteration: {out}")
     return {"ms_per_iter": out}
+
+
+def run_table_gather(sf, dev, n=64, p=P, seed=7):
+    """The unstructured (cell-to-dof table) gather: the Q4 64^3 problem with its free
+    dofs randomly renumbered, so that sf_set_cells' table (int32 per cell and local
+    dof) drives the general element kernel's gather and atomic scatter. FP64 and
+    FP32 apply times and bytes moved, beside the tiled kernel on the same mesh."""
+    import torch
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n))
+    m = sf.SumFactorizationMap(3, (p,) * 3, (DEG,) * 3)
+    t0 = time.perf_counter()
+    V = sf.FESpace(model, p, renumber_seed=seed)
+    A = sf.LazyMatrix(m, V, V, sf.Measure(model, DEG))
+    setup_s = time.perf_counter() - t0
+    assert not A.uses_tiled_kernel()
+    x = torch.from_numpy(np.random.default_rng(seed).uniform(-1, 1, A.n)).to(dev)
+    y = torch.empty_like(x)
+    ndof = (n * p + 1) ** 3
+    ids_bytes = n ** 3 * (p + 1) ** 3 * 4
+    res = {"mesh": f"{n}^3 Q{p}, {DEG}-degree Gauss, free dofs renumbered (seed {seed})",
+           "n_free": A.n, "setup_s": round(setup_s, 2), "kernel": A.kernel_name(),
+           "table_bytes": ids_bytes}
+    for dt, key, vb in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
+        xx, yy = x.to(dt), y.to(dt)
+        for _ in range(3):
+            sf.mul(yy, A, xx)
+        ms = _events_ms(lambda: sf.mul(yy, A, xx), 10)
+        byts = ids_bytes + ndof * 2 * vb
+        res[key] = {"ms": round(ms, 3), "gdof_s": round(ndof / (ms * 1e-3) / 1e9, 2),
+                    "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1)}
+    log(f"table gather apply: {res}")
+    return res
 
 
 def run_quad2d(sf, dev, n=1024, orders=(4, 5, 6, 7)):
