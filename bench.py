@@ -715,33 +715,35 @@ def run_cg_fused(sf, dev, candidate=None, maxiter=6000):
 
 
 def run_table_gather(sf, dev, n=64, p=P, seed=7):
-    """The unstructured (cell-to-dof table) gather: the Q4 64^3 problem with its free
-    dofs randomly renumbered, so that sf_set_cells' table (int32 per cell and local
-    dof) drives the general element kernel's gather and atomic scatter. FP64 and
-    FP32 apply times and bytes moved, beside the tiled kernel on the same mesh."""
+    """The unstructured (cell-to-dof table) gather: the Q4 64^3 problem driven by
+    sf_set_cells' table (int32 per cell and local dof) through the general element
+    kernel's gather and atomic scatter, with the lexicographic numbering (cells
+    near in the table are near in the vectors) and with the free dofs randomly
+    renumbered (no locality: the worst case). FP64 and FP32 apply times and bytes
+    moved; the tiled kernel does the same mesh in about 0.123 ms (FP64)."""
     import torch
     model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n))
     m = sf.SumFactorizationMap(3, (p,) * 3, (DEG,) * 3)
-    t0 = time.perf_counter()
-    V = sf.FESpace(model, p, renumber_seed=seed)
-    A = sf.LazyMatrix(m, V, V, sf.Measure(model, DEG))
-    setup_s = time.perf_counter() - t0
-    assert not A.uses_tiled_kernel()
-    x = torch.from_numpy(np.random.default_rng(seed).uniform(-1, 1, A.n)).to(dev)
-    y = torch.empty_like(x)
     ndof = (n * p + 1) ** 3
     ids_bytes = n ** 3 * (p + 1) ** 3 * 4
-    res = {"mesh": f"{n}^3 Q{p}, {DEG}-degree Gauss, free dofs renumbered (seed {seed})",
-           "n_free": A.n, "setup_s": round(setup_s, 2), "kernel": A.kernel_name(),
-           "table_bytes": ids_bytes}
-    for dt, key, vb in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
-        xx, yy = x.to(dt), y.to(dt)
-        for _ in range(3):
-            sf.mul(yy, A, xx)
-        ms = _events_ms(lambda: sf.mul(yy, A, xx), 10)
-        byts = ids_bytes + ndof * 2 * vb
-        res[key] = {"ms": round(ms, 3), "gdof_s": round(ndof / (ms * 1e-3) / 1e9, 2),
-                    "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1)}
+    res = {"mesh": f"{n}^3 Q{p}, {DEG}-degree Gauss", "table_bytes": ids_bytes}
+    for numbering, rseed in (("lexicographic", None), ("random", seed)):
+        V = sf.FESpace(model, p, renumber_seed=rseed)
+        A = sf.LazyMatrix(m, V, V, sf.Measure(model, DEG), gather="table")
+        assert not A.uses_tiled_kernel()
+        x = torch.from_numpy(np.random.default_rng(seed).uniform(-1, 1, A.n)).to(dev)
+        y = torch.empty_like(x)
+        out = {"kernel": A.kernel_name()}
+        for dt, key, vb in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
+            xx, yy = x.to(dt), y.to(dt)
+            for _ in range(3):
+                sf.mul(yy, A, xx)
+            ms = _events_ms(lambda: sf.mul(yy, A, xx), 10)
+            byts = ids_bytes + ndof * 2 * vb
+            out[key] = {"ms": round(ms, 3), "gdof_s": round(ndof / (ms * 1e-3) / 1e9, 2),
+                        "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1)}
+        res[numbering] = out
+        del A, x, y
     log(f"table gather apply: {res}")
     return res
 
