@@ -98,6 +98,23 @@ int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* 
 int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_order);
 
 /*
+ * sf_set_structured with the caller's own numbering of the free dofs:
+ * free_id[i] (0-based) is the caller's id of lexicographic free point i
+ * (x fastest over the (nx p - 1)(ny p - 1)(nz p - 1) interior grid points), a
+ * permutation of 0 .. n_free-1. This is the Cartesian mesh of the reference's
+ * drivers with Gridap's own dof numbering (get_cell_dof_ids,
+ * src/LazyMatrices.jl:46), which is not lexicographic. The tiled kernels still
+ * run: sf_apply, sf_apply_multi and sf_mul_host permute x into lexicographic
+ * order and the result back (two extra vector sweeps per apply); sf_cg permutes
+ * b and x once per solve and iterates in lexicographic order; sf_diagonal and
+ * sf_rhs compute lexicographically and permute the result. sf_kappa_vjp, the
+ * sf_cgd_* steps, sf_cg_noalloc and the batched form reject such a handle.
+ * 3D only. sf_set_cells or sf_set_structured drops the numbering.
+ */
+int sf_set_structured_numbering(sf_op* op, int nx, int ny, int nz, const int32_t* node_order,
+                                const int32_t* free_id);
+
+/*
  * The z-slab of cells [z0, z1) of an nx x ny x nz structured mesh (the share of
  * one rank when the mesh is split along z; the reference's Gridap model is one
  * process, so this has no single counterpart there). Vectors of a slab
@@ -272,6 +289,7 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *   "owned_offset", "owned_count": the points sf_apply writes (the whole vector
  *                              unless the operator is a slab)
  *   "jacobi_table"           : 1 if sf_cg's FP64 Jacobi mode reads D^-1 from the table
+ *   "numbered"               : 1 after sf_set_structured_numbering
  *   "cg_fused"               : 1 if sf_cg's FP64 modes use the fused CG kernel
  *   "cg_candidates"          : number of tile shapes of the fused CG kernel
  */

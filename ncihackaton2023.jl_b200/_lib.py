@@ -75,6 +75,7 @@ SIGNATURES = {
     "sf_kernel_name": (C.c_char_p, [vp, i32]),
     "sf_cg_kernel_name": (C.c_char_p, [vp]),
     "sf_set_structured_slab": (i32, [vp, i32, i32, i32, i32, i32, vp]),
+    "sf_set_structured_numbering": (i32, [vp, i32, i32, i32, vp, vp]),
     "sf_rhs": (i32, [vp, vp, vp, vp]),
     "sf_cgd_start": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "sf_cgd_init": (i32, [vp, vp, C.c_double, vp]),

@@ -45,6 +45,11 @@ struct sf_op {
   int slab_z0 = 0, slab_z1 = 0, mesh_nz = 0;
   long long plane = 0;       // free points per z level
   double* d_dinv = nullptr;  // 1 / diag(A) on the owned points (distributed CG)
+  // sf_set_structured_numbering: the caller's free id of each lexicographic free point.
+  // Vector entry points then permute into lexicographic order and back around the work.
+  int32_t* d_numbering = nullptr;
+  void* d_lex = nullptr;     // two lexicographic vectors (8 bytes per entry) for that
+  bool lex_inside = false;   // set while the work runs on lexicographic vectors
   // workspaces
   double* d_diag = nullptr;  // FP64 diag(A), cached
   double* d_jtab = nullptr;  // inverse Jacobi diagonal per position in a cell (Cartesian), cached
@@ -89,6 +94,11 @@ int guarded(sf_op* op, F&& f) {
   } catch (const std::exception& e) {
     return fail(op, SF_ERR_ARG, e.what());
   }
+}
+
+// Rethrows the failure of a nested entry-point call on the same handle.
+void check_status(int status, const sf_op* op) {
+  if (status != SF_OK) throw Error(status, op->err);
 }
 
 void dfree(void* p) {
@@ -166,12 +176,54 @@ void update_cartesian(sf_op* op) {
   op->cart.slab_top = op->slab && op->slab_z1 == op->mesh_nz;
 }
 
+// A numbered operator whose caller passes vectors in its own numbering.
+bool numbered(const sf_op* op) { return op->d_numbering && !op->lex_inside; }
+
+// Lexicographic vector k (0 or 1) of a numbered operator, n_free entries of up to 8 bytes.
+void* lex_vec(sf_op* op, int k) {
+  const size_t vb = (op->n_free * sizeof(double) + 255) & ~size_t(255);
+  if (!op->d_lex) SF_CUDA_CHECK(cudaMalloc(&op->d_lex, 2 * vb));
+  return static_cast<char*>(op->d_lex) + k * vb;
+}
+
+// While alive, vector entry points take lexicographic vectors.
+struct LexScope {
+  sf_op* op;
+  bool prev;
+  explicit LexScope(sf_op* o) : op(o), prev(o->lex_inside) { o->lex_inside = true; }
+  ~LexScope() { op->lex_inside = prev; }
+};
+
+void drop_numbering(sf_op* op) {
+  dfree(op->d_numbering);
+  op->d_numbering = nullptr;
+  dfree(op->d_lex);
+  op->d_lex = nullptr;
+}
+
+void require_own_numbering(const sf_op* op, const char* what) {
+  SF_REQUIRE(!op->d_numbering, SF_ERR_UNSUPPORTED,
+             std::string(what) + " does not take an operator with a dof numbering "
+                                 "(sf_set_structured_numbering)");
+}
+
 void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
   require_ready(op);
   const size_t es = dsize(dtype);
   if (op->n_free == 0) return;
   SF_REQUIRE(x && y, SF_ERR_ARG, "null x or y");
   SF_REQUIRE(x != y, SF_ERR_ARG, "x and y must not alias");
+  if (numbered(op)) {  // into lexicographic order, apply, back
+    void* xl = lex_vec(op, 0);
+    void* yl = lex_vec(op, 1);
+    sf::permute_gather(dtype, x, op->d_numbering, xl, op->n_free, st);
+    {
+      LexScope lex(op);
+      apply_impl(op, dtype, xl, yl, st);
+    }
+    sf::permute_scatter(dtype, yl, op->d_numbering, y, op->n_free, st);
+    return;
+  }
   if (op->cartesian_ok && sf::cartesian_supported(op->cart, dtype)) {
     sf::cartesian_apply(op->cart, dtype, x, y, st);
     return;
@@ -232,7 +284,8 @@ bool host_pinned(const void* p) {
 // its tiles read (up to one cell above its last row) are on the device, and its
 // owned levels go back as soon as it is done. Returns false when it does not apply.
 bool mul_host_pipelined(sf_op* op, const double* x, double* y) {
-  if (!(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64)) || op->slab || op->D != 3)
+  if (!(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64)) || op->slab || op->D != 3 ||
+      op->d_numbering)
     return false;
   if (!host_pinned(x) || !host_pinned(y)) return false;
   const int P = op->p, nz = op->cells.nz;
@@ -745,6 +798,7 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_diag);
   dfree(op->d_jtab);
   dfree(op->d_dinv);
+  drop_numbering(op);
   dfree(op->d_ws);
   dfree(op->d_hx);
   dfree(op->d_hy);
@@ -795,6 +849,7 @@ int sf_set_cells(sf_op* op, int64_t ncells, const int32_t* ptrs, const int32_t* 
       }
     }
     dfree(op->d_ids);
+    drop_numbering(op);
     op->d_ids = nullptr;
     op->d_ids = dalloc<int32_t>(ids.size());
     SF_CUDA_CHECK(cudaMemcpy(op->d_ids, ids.data(), ids.size() * sizeof(int32_t),
@@ -828,6 +883,7 @@ int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_ord
     rebuild_kernel_basis(op);
     dfree(op->d_ids);
     op->d_ids = nullptr;
+    drop_numbering(op);
     op->cells = sf::Cells();
     op->cells.mesh = sf::MESH_STRUCTURED;
     op->cells.ncells = (long long)nx * ny * (op->D == 2 ? 1 : nz);
@@ -861,6 +917,28 @@ int sf_set_structured_slab(sf_op* op, int nx, int ny, int nz, int z0, int z1,
     SF_REQUIRE(op->n_free < (1LL << 31), SF_ERR_ARG, "slab too large for int32 dof ids");
     invalidate_caches(op);
     update_cartesian(op);
+  });
+}
+
+int sf_set_structured_numbering(sf_op* op, int nx, int ny, int nz, const int32_t* node_order,
+                                const int32_t* free_id) {
+  if (!op) return SF_ERR_ARG;
+  if (op->D != 3) return fail(op, SF_ERR_UNSUPPORTED, "sf_set_structured_numbering is 3D only");
+  if (!free_id) return fail(op, SF_ERR_ARG, "null free_id");
+  const int status = sf_set_structured(op, nx, ny, nz, node_order);
+  if (status != SF_OK) return status;
+  return guarded(op, [&] {
+    const long long n = op->n_free;
+    std::vector<char> seen((size_t)n, 0);
+    for (long long i = 0; i < n; ++i) {
+      const int32_t k = free_id[i];
+      SF_REQUIRE(k >= 0 && k < n && !seen[(size_t)k], SF_ERR_ARG,
+                 "free_id must be a permutation of 0 .. n_free-1 (entry " + std::to_string(i) + ")");
+      seen[(size_t)k] = 1;
+    }
+    op->d_numbering = dalloc<int32_t>((size_t)n);
+    SF_CUDA_CHECK(cudaMemcpy(op->d_numbering, free_id, (size_t)n * sizeof(int32_t),
+                             cudaMemcpyHostToDevice));
   });
 }
 
@@ -1007,6 +1085,7 @@ int sf_kappa_vjp(sf_op* op, int dtype, const void* x, const void* ybar, double* 
   return guarded(op, [&] {
     require_ready(op);
     SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_kappa_vjp does not take slab operators");
+    require_own_numbering(op, "sf_kappa_vjp");
     SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "sf_kappa_vjp is 3D only");
     SF_REQUIRE(x && ybar && kappa_bar, SF_ERR_ARG, "null x, ybar or kappa_bar");
     sf::launch_kappa_vjp(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, x,
@@ -1083,6 +1162,15 @@ int sf_rhs(sf_op* op, const double* fq, double* b, void* stream) {
     SF_REQUIRE(!op->slab, SF_ERR_UNSUPPORTED, "sf_rhs does not take slab operators");
     SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "sf_rhs is 3D only");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (numbered(op)) {  // in lexicographic order, then into the caller's numbering
+      double* bl = static_cast<double*>(lex_vec(op, 0));
+      {
+        LexScope lex(op);
+        check_status(sf_rhs(op, fq, bl, stream), op);
+      }
+      sf::permute_scatter(SF_F64, bl, op->d_numbering, b, op->n_free, st);
+      return;
+    }
     SF_CUDA_CHECK(cudaMemsetAsync(b, 0, op->n_free * sizeof(double), st));
     sf::launch_general_rhs(op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom, fq, b,
                            st);
@@ -1096,6 +1184,15 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream) {
     SF_REQUIRE(d, SF_ERR_ARG, "null d");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t es = dsize(dtype);
+    if (numbered(op)) {  // in lexicographic order, then into the caller's numbering
+      void* dl = lex_vec(op, 0);
+      {
+        LexScope lex(op);
+        check_status(sf_diagonal(op, dtype, dl, stream), op);
+      }
+      sf::permute_scatter(dtype, dl, op->d_numbering, d, op->n_free, st);
+      return;
+    }
     if (op->slab || op->D == 2) {
       SF_REQUIRE(dtype == SF_F64, SF_ERR_UNSUPPORTED,
                  "the diagonal of a slab or 2D operator is FP64");
@@ -1118,14 +1215,30 @@ int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int ma
     SF_REQUIRE(b && x, SF_ERR_ARG, "null b or x");
     SF_REQUIRE(reltol > 0 && maxiter >= 0, SF_ERR_ARG, "bad reltol / maxiter");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SF_REQUIRE(mode == SF_CG_F64 || mode == SF_CG_F64_PLAIN || mode == SF_CG_MIXED, SF_ERR_ARG,
+               "unknown CG mode");
     double rel = 0.0;
     int it = 0, outer = 1;
-    if (mode == SF_CG_F64 || mode == SF_CG_F64_PLAIN)
-      it = cg_f64(op, mode == SF_CG_F64, b, x, reltol, maxiter, &rel, st);
-    else if (mode == SF_CG_MIXED)
-      it = cg_mixed(op, b, x, reltol, maxiter, &rel, &outer, st);
-    else
-      throw Error(SF_ERR_ARG, "unknown CG mode");
+    // a numbered operator solves in lexicographic order: b and x are permuted once
+    const bool perm = numbered(op);
+    const double* bs = b;
+    double* xs = x;
+    if (perm) {
+      double* bl = static_cast<double*>(lex_vec(op, 0));
+      double* xl = static_cast<double*>(lex_vec(op, 1));
+      sf::permute_gather(SF_F64, b, op->d_numbering, bl, op->n_free, st);
+      sf::permute_gather(SF_F64, x, op->d_numbering, xl, op->n_free, st);
+      bs = bl;
+      xs = xl;
+    }
+    {
+      LexScope lex(op);  // no effect without a numbering
+      if (mode == SF_CG_MIXED)
+        it = cg_mixed(op, bs, xs, reltol, maxiter, &rel, &outer, st);
+      else
+        it = cg_f64(op, mode == SF_CG_F64, bs, xs, reltol, maxiter, &rel, st);
+    }
+    if (perm) sf::permute_scatter(SF_F64, xs, op->d_numbering, x, op->n_free, st);
     op->last_inner = it;
     op->last_outer = outer;
     op->last_relres = rel;
@@ -1150,6 +1263,7 @@ int sf_cgd_start(sf_op* op, const double* b, const double* x, double* r, double*
   return guarded(op, [&] {
     require_ready(op);
     SF_REQUIRE(b && x && r && p && q && s, SF_ERR_ARG, "null vector or scalar block");
+    require_own_numbering(op, "sf_cgd_start");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long off = owned_offset(op), n = owned_count(op);
     const double* dinv = ensure_dinv(op, st);
@@ -1173,6 +1287,7 @@ int sf_cgd_apply(sf_op* op, const double* p, double* q, double* s, void* stream)
   return guarded(op, [&] {
     require_ready(op);
     SF_REQUIRE(p && q && s, SF_ERR_ARG, "null p, q or scalar block");
+    require_own_numbering(op, "sf_cgd_apply");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     double* partials = static_cast<double*>(workspace(op, cg_partials(op) * sizeof(double)));
     if (tiled(op, SF_F64)) {
@@ -1193,6 +1308,7 @@ int sf_cgd_update(sf_op* op, double* r, const double* q, double* s, void* stream
   return guarded(op, [&] {
     require_ready(op);
     SF_REQUIRE(r && q && s, SF_ERR_ARG, "null r, q or scalar block");
+    require_own_numbering(op, "sf_cgd_update");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long off = owned_offset(op), n = owned_count(op);
     const double* dinv = ensure_dinv(op, st);
@@ -1206,6 +1322,7 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
   return guarded(op, [&] {
     require_ready(op);
     SF_REQUIRE(x && p && r && s, SF_ERR_ARG, "null x, p, r or scalar block");
+    require_own_numbering(op, "sf_cgd_direction");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const long long off = owned_offset(op), n = owned_count(op);
     const double* dinv = ensure_dinv(op, st);
@@ -1318,6 +1435,7 @@ int sf_get_info(const sf_op* op, const char* key, double* value) {
   else if (k == "geometry_kind") *value = (double)op->geom.kind;
   else if (k == "slab") *value = op->slab ? 1.0 : 0.0;
   else if (k == "cg_fused") *value = use_fused_cg(op) ? 1.0 : 0.0;
+  else if (k == "numbered") *value = op->d_numbering ? 1.0 : 0.0;
   else if (k == "jacobi_table")
     *value = (op->jacobi_table && !op->slab && tiled && op->D == 3) ? 1.0 : 0.0;
   else if (k == "cg_candidates") *value = (double)sf::cartesian_cg_candidates(op->cart);
@@ -1446,6 +1564,7 @@ extern "C" int sf_cg_noalloc(sf_op* op, int mode, const double* b, double* x, do
     require_ready(op);
     SF_REQUIRE(b && x, SF_ERR_ARG, "null b or x");
     SF_REQUIRE(reltol > 0 && maxiter >= 0, SF_ERR_ARG, "bad reltol / maxiter");
+    require_own_numbering(op, "sf_cg_noalloc");
     SF_REQUIRE(op->n_free <= kNoAllocMaxFree, SF_ERR_ARG,
                "n_free = " + std::to_string(op->n_free) +
                    " exceeds the no-alloc scratch limit SF_NOALLOC_MAX_FREE = " +
@@ -1642,6 +1761,7 @@ extern "C" int sf_batch_create(sf_batch** out, int nops, sf_op* const* ops, int 
       SF_REQUIRE(op, SF_ERR_ARG, "null handle in the batch");
       require_ready(op);
       SF_REQUIRE(op->D == 3, SF_ERR_UNSUPPORTED, "the batched form takes 3D operators");
+      require_own_numbering(op, "the batched form");
       SF_REQUIRE(op->cartesian_ok && sf::cartesian_supported(op->cart, SF_F64), SF_ERR_UNSUPPORTED,
                  "batch member " + std::to_string(i) +
                      " is not a constant-coefficient Cartesian problem (tiled kernel)");

@@ -102,8 +102,11 @@ class LazyMatrix:
     ``gather`` selects how cells find their dofs: "structured" uses the
     implicit lexicographic numbering of the Cartesian model (the tiled
     kernels). "table" uploads get_cell_dof_ids as a Gridap Table, so that any
-    global numbering works. A space with a renumbered global numbering always
-    uses the table."""
+    global numbering works; a space with a renumbered global numbering uses
+    the table unless "numbered" is asked for. "numbered" keeps the structured
+    (tiled) kernels for a renumbered space of a Cartesian model: vectors in the
+    space's numbering are permuted into lexicographic order and back around
+    each apply, and once per solve in cg (sf_set_structured_numbering)."""
 
     def __init__(self, m: SumFactorizationMap, trial: fem.FESpace, test: fem.FESpace,
                  dOmega: fem.Measure, gather: str = "structured"):
@@ -118,7 +121,10 @@ class LazyMatrix:
         self.test = test
         self.model = test.model
         self.n = test.num_free_dofs
-        self.gather = "table" if test.perm is not None else gather
+        if gather == "numbered":
+            self.gather = "numbered"
+        else:
+            self.gather = "table" if test.perm is not None else gather
         self._h = m._create_handle()
         try:
             if m.D != self.model.D:
@@ -127,13 +133,21 @@ class LazyMatrix:
                 part = tuple(self.model.partition) + ((0,) if m.D == 2 else ())
                 no = _i32(m.node_order)
                 check(lib.sf_set_structured(self._h, *part, _ptr(no)), self._h, "sf_set_structured")
+            elif self.gather == "numbered":
+                if m.D != 3:
+                    raise NotImplementedError("gather='numbered' is 3D only")
+                no = _i32(m.node_order)
+                ids = _i32(test.perm if test.perm is not None else np.arange(self.n))
+                check(lib.sf_set_structured_numbering(self._h, *tuple(self.model.partition),
+                                                      _ptr(no), _ptr(ids)),
+                      self._h, "sf_set_structured_numbering")
             elif self.gather == "table":
                 t = test.get_cell_dof_ids()
                 ptrs, data = _i32(t.ptrs), _i32(t.data)
                 check(lib.sf_set_cells(self._h, len(t), _ptr(ptrs), _ptr(data), self.n), self._h,
                       "sf_set_cells")
             else:
-                raise ValueError("gather must be 'structured' or 'table'")
+                raise ValueError("gather must be 'structured', 'table' or 'numbered'")
             fill, wq, jq, djq = fem.cell_quantities(self.model, m.points, m.weights)
             self.cell_quantities = (fill, wq, jq, djq)
             wq, jq, djq = _f64(wq), _f64(jq), _f64(djq)
