@@ -59,7 +59,8 @@ def test_numbered_diagonal_and_rhs_match_table(sf):
         d_ref = A_tab.diagonal(dt)
         assert (d.double() - d_ref.double()).abs().max().item() <= 1e-6 * d_ref.abs().max().item()
     d = A_num.diagonal()
-    assert torch.equal(d[perm], A_lex.diagonal())
+    d_lex = A_lex.diagonal()  # assembled with atomics: equal up to the order of the sums
+    assert (d[perm] - d_lex).abs().max().item() <= 1e-13 * d_lex.abs().max().item()
     X = sf.quadrature_points(A_num)
     f = 3 * np.pi ** 2 * torch.prod(torch.sin(np.pi * X), dim=-1)
     b = sf.rhs(A_num, f)
