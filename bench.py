@@ -722,7 +722,7 @@ def run_table_gather(sf, dev, n=64, p=P, seed=7):
     renumbered (no locality: the worst case); and the random numbering through
     sf_set_structured_numbering instead (the tiled kernel between a permutation of
     x in and of y out). FP64 and FP32 apply times and bytes moved; the tiled kernel
-    does the lexicographic mesh in about 0.123 ms (FP64).
+    does the lexicographic mesh in about 0.123 ms (FP64)."""
     import torch
     model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n))
     m = sf.SumFactorizationMap(3, (p,) * 3, (DEG,) * 3)
