@@ -719,7 +719,8 @@ def run_table_gather(sf, dev, n=64, p=P, seed=7):
     sf_set_cells' table (int32 per cell and local dof) through the general element
     kernel's gather and atomic scatter, with the lexicographic numbering (cells
     near in the table are near in the vectors) and with the free dofs randomly
-    renumbered (no locality: the worst case); and the random numbering through
+    renumbered (no locality: the worst case), and numbered cell by cell (as a
+    finite-element library numbers its spaces); and these numberings through
     sf_set_structured_numbering instead (the tiled kernel between a permutation of
     x in and of y out). FP64 and FP32 apply times and bytes moved; the tiled kernel
     does the lexicographic mesh in about 0.123 ms (FP64)."""
@@ -730,10 +731,15 @@ def run_table_gather(sf, dev, n=64, p=P, seed=7):
     ids_bytes = n ** 3 * (p + 1) ** 3 * 4
     res = {"mesh": f"{n}^3 Q{p}, {DEG}-degree Gauss", "table_bytes": ids_bytes}
     for numbering, rseed, gather in (("lexicographic", None, "table"), ("random", seed, "table"),
-                                     ("random_numbered", seed, "numbered")):
-        # "numbered": the same random numbering through sf_set_structured_numbering (the
-        # tiled kernel on permuted vectors; no table)
-        V = sf.FESpace(model, p, renumber_seed=rseed)
+                                     ("random_numbered", seed, "numbered"),
+                                     ("cellwise", "cellwise", "table"),
+                                     ("cellwise_numbered", "cellwise", "numbered")):
+        # "numbered": the same numbering through sf_set_structured_numbering (the tiled
+        # kernel on permuted vectors; no table). "cellwise": free dofs numbered cell by cell
+        if rseed == "cellwise":
+            V = sf.FESpace(model, p, cellwise=True)
+        else:
+            V = sf.FESpace(model, p, renumber_seed=rseed)
         A = sf.LazyMatrix(m, V, V, sf.Measure(model, DEG), gather=gather)
         assert A.uses_tiled_kernel() == (gather == "numbered")
         x = torch.from_numpy(np.random.default_rng(seed).uniform(-1, 1, A.n)).to(dev)

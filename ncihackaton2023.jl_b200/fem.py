@@ -185,13 +185,17 @@ class FESpace:
     whole boundary (``dirichlet_tags=["boundary"]``, profiling/drivers.jl:15-16).
     Free dofs are numbered lexicographically (x fastest) over the interior dof
     grid; Dirichlet dofs get negative ids. ``renumber_seed`` applies a seeded
-    random permutation to the free ids (an arbitrary global numbering, as a
-    Gridap space would have)."""
+    random permutation to the free ids (an arbitrary global numbering, with no
+    locality). ``cellwise`` numbers the free dofs instead in the order in which
+    they first appear going through the cells in order, each cell in its local
+    dof order: a cell-by-cell numbering such as a finite-element library gives
+    its spaces (locality kept)."""
 
     model: CartesianDiscreteModel
     order: int
     dirichlet_tags: str = "boundary"
     renumber_seed: int | None = None
+    cellwise: bool = False
 
     def __post_init__(self):
         if self.dirichlet_tags != "boundary":
@@ -201,9 +205,19 @@ class FESpace:
         self.free_grid = tuple(n * p - 1 for n in self.model.partition)
         self._ids = None
         self.perm = None
+        if self.renumber_seed is not None and self.cellwise:
+            raise ValueError("renumber_seed and cellwise are exclusive")
         if self.renumber_seed is not None:
             self.perm = (np.random.default_rng(self.renumber_seed)
                          .permutation(self.num_free_dofs).astype(np.int64))
+        elif self.cellwise:
+            data = np.asarray(self.get_cell_dof_ids().data)  # lexicographic ids, cell by cell
+            free = data[data > 0]
+            lex, first = np.unique(free, return_index=True)
+            perm = np.empty(self.num_free_dofs, dtype=np.int64)
+            perm[lex[np.argsort(first, kind="stable")] - 1] = np.arange(lex.size)
+            self.perm = perm
+            self._ids = None
 
     @property
     def num_free_dofs(self) -> int:

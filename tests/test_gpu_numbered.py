@@ -114,3 +114,14 @@ def test_identity_numbering_equals_structured(sf):
     A = sf.LazyMatrix(m, V, V, sf.Measure(model, 6))
     x = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, A.n)).cuda()
     assert torch.equal(A_id @ x, A @ x)
+
+
+def test_cellwise_numbering_matches_table(sf):
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (4, 5, 3))
+    m = sf.SumFactorizationMap(3, (4,) * 3, (8,) * 3)
+    V = sf.FESpace(model, 4, cellwise=True)
+    A_num = sf.LazyMatrix(m, V, V, sf.Measure(model, 8), gather="numbered")
+    A_tab = sf.LazyMatrix(m, V, V, sf.Measure(model, 8), gather="table")
+    x = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, A_num.n)).cuda()
+    y_ref = A_tab @ x
+    assert ((A_num @ x) - y_ref).abs().max().item() <= 1e-12 * y_ref.abs().max().item()

@@ -83,3 +83,22 @@ def test_free_dof_coordinates(sf):
     om = O.make_map(3, 2, 4)
     mesh = O.cartesian_mesh(3, (2, 3, 4), 2, om)
     assert np.allclose(V.free_dof_coordinates(), O.free_dof_coordinates(mesh))
+
+
+def test_cellwise_numbering(sf):
+    """Cell-by-cell numbering: a permutation; the first cell's free dofs come first,
+    in local order; the table of the renumbered space is the permuted lexicographic one."""
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (3, 4, 2))
+    V = sf.FESpace(model, 3, cellwise=True)
+    L = sf.FESpace(model, 3)
+    n = V.num_free_dofs
+    assert np.array_equal(np.sort(V.perm), np.arange(n))
+    dv = np.asarray(V.get_cell_dof_ids().data)
+    dl = np.asarray(L.get_cell_dof_ids().data)
+    free = dl > 0
+    assert np.array_equal(dv[free], V.perm[dl[free] - 1] + 1)
+    assert np.array_equal(dv[~free], dl[~free])
+    first = dv[:64][dv[:64] > 0]
+    assert np.array_equal(first, np.arange(1, first.size + 1))
+    with pytest.raises(ValueError):
+        sf.FESpace(model, 3, cellwise=True, renumber_seed=1)
