@@ -417,7 +417,8 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_secondary and world == 1 and NCELL == 64:
         t_sec = time.perf_counter()
         for key, fn in (("batched", run_batched), ("adjoint", run_adjoint),
-                        ("deformed_q8", run_deformed), ("quad2d", run_quad2d)):
+                        ("deformed_q8", run_deformed), ("quad2d", run_quad2d),
+                        ("table_gather", run_table_gather)):
             if time.perf_counter() - t_sec > SECONDARY_BUDGET_S:
                 out[key] = {"skipped": "secondary time budget spent"}
                 continue
