@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-secondary", action="store_true",
-                    help="skip the batched, adjoint and deformed-mesh sections")
+                    help="skip the batched, adjoint, deformed-mesh, 2D and table-gather sections")
     ap.add_argument("--tile", type=int, default=None,
                     help="force tile candidate K of the FP64 tiled kernel (skips the autotuner)")
     ap.add_argument("--cg-candidate", type=int, default=None,
