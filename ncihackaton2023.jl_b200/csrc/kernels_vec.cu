@@ -467,9 +467,9 @@ __global__ void k_cg_direction_table(double* __restrict__ s, T* __restrict__ x,
   }
 }
 
-// y[i] = x[idx[i]] (GATHER) or y[idx[i]] = x[i]; the index stream and one side are
-// coalesced, kUnroll entries per thread in flight.
-template <typename T, bool GATHER>
+// y[i] = x[idx[i]]: the index stream and y are coalesced, kUnroll entries per thread
+// in flight.
+template <typename T>
 __global__ void k_permute(const T* __restrict__ x, const int32_t* __restrict__ idx,
                           T* __restrict__ y, long long n) {
   const long long S = (long long)gridDim.x * kThreads;
@@ -480,17 +480,11 @@ __global__ void k_permute(const T* __restrict__ x, const int32_t* __restrict__ i
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) k[u] = idx[i + u * S];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) v[u] = GATHER ? x[k[u]] : x[i + u * S];
+    for (int u = 0; u < kUnroll; ++u) v[u] = x[k[u]];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      if (GATHER) y[i + u * S] = v[u];
-      else y[k[u]] = v[u];
-    }
+    for (int u = 0; u < kUnroll; ++u) y[i + u * S] = v[u];
   }
-  for (; i < n; i += S) {
-    if (GATHER) y[i] = x[idx[i]];
-    else y[idx[i]] = x[i];
-  }
+  for (; i < n; i += S) y[i] = x[idx[i]];
 }
 
 __global__ void k_copy_scalar(double* __restrict__ s, int dst, int src) {
@@ -674,31 +668,19 @@ void cg_direction_table(double* s, T* x, T* p, const T* r, const JacobiTable& J,
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-namespace {
-template <bool GATHER>
-void permute(int dtype, const void* x, const int32_t* idx, void* y, long long n, cudaStream_t st) {
+void permute_gather(int dtype, const void* x, const int32_t* idx, void* y, long long n,
+                    cudaStream_t st) {
   if (n <= 0) return;
   if (dtype == SF_F64) {
-    k_permute<double, GATHER><<<grid_for(k_permute<double, GATHER>, n), kThreads, 0, st>>>(
+    k_permute<double><<<grid_for(k_permute<double>, n), kThreads, 0, st>>>(
         static_cast<const double*>(x), idx, static_cast<double*>(y), n);
   } else if (dtype == SF_F32) {
-    k_permute<float, GATHER><<<grid_for(k_permute<float, GATHER>, n), kThreads, 0, st>>>(
+    k_permute<float><<<grid_for(k_permute<float>, n), kThreads, 0, st>>>(
         static_cast<const float*>(x), idx, static_cast<float*>(y), n);
   } else {
     throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
   }
   SF_CUDA_CHECK(cudaGetLastError());
-}
-}  // namespace
-
-void permute_gather(int dtype, const void* x, const int32_t* idx, void* y, long long n,
-                    cudaStream_t st) {
-  permute<true>(dtype, x, idx, y, n, st);
-}
-
-void permute_scatter(int dtype, const void* x, const int32_t* idx, void* y, long long n,
-                     cudaStream_t st) {
-  permute<false>(dtype, x, idx, y, n, st);
 }
 
 void cg_fused_finish(double* s, const double* partials, long long ntiles, bool first,

@@ -93,12 +93,10 @@ void cg_direction_table(double* s, T* x, T* p, const T* r, const JacobiTable& J,
 void cg_fused_finish(double* s, const double* partials, long long ntiles, bool first,
                      double* report, cudaStream_t st);
 
-// Permutations of a vector of dtype SF_F64 / SF_F32 (n entries, idx a permutation of 0..n-1):
-// gather y[i] = x[idx[i]]; scatter y[idx[i]] = x[i].
+// y[i] = x[idx[i]] for a vector of dtype SF_F64 / SF_F32 (n entries, idx a permutation
+// of 0..n-1; the inverse permutation undoes it).
 void permute_gather(int dtype, const void* x, const int32_t* idx, void* y, long long n,
                     cudaStream_t st);
-void permute_scatter(int dtype, const void* x, const int32_t* idx, void* y, long long n,
-                     cudaStream_t st);
 // Reliable update: r32 = float(b - q), xs32 = 0, optionally p32 = dinv r32;
 // writes s[CG_RZ_NEW] = (r32, dinv r32) and s[CG_RR] = FP64 (r, r).
 void mixed_residual(const double* b, const double* q, const float* dinv, float* r32, float* xs32,

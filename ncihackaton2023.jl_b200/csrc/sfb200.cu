@@ -48,6 +48,7 @@ struct sf_op {
   // sf_set_structured_numbering: the caller's free id of each lexicographic free point.
   // Vector entry points then permute into lexicographic order and back around the work.
   int32_t* d_numbering = nullptr;
+  int32_t* d_numbering_inv = nullptr;  // its inverse: lexicographic index of each caller id
   void* d_lex = nullptr;     // two lexicographic vectors (8 bytes per entry) for that
   bool lex_inside = false;   // set while the work runs on lexicographic vectors
   // workspaces
@@ -197,6 +198,8 @@ struct LexScope {
 void drop_numbering(sf_op* op) {
   dfree(op->d_numbering);
   op->d_numbering = nullptr;
+  dfree(op->d_numbering_inv);
+  op->d_numbering_inv = nullptr;
   dfree(op->d_lex);
   op->d_lex = nullptr;
 }
@@ -221,7 +224,7 @@ void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
       LexScope lex(op);
       apply_impl(op, dtype, xl, yl, st);
     }
-    sf::permute_scatter(dtype, yl, op->d_numbering, y, op->n_free, st);
+    sf::permute_gather(dtype, yl, op->d_numbering_inv, y, op->n_free, st);
     return;
   }
   if (op->cartesian_ok && sf::cartesian_supported(op->cart, dtype)) {
@@ -936,8 +939,15 @@ int sf_set_structured_numbering(sf_op* op, int nx, int ny, int nz, const int32_t
                  "free_id must be a permutation of 0 .. n_free-1 (entry " + std::to_string(i) + ")");
       seen[(size_t)k] = 1;
     }
+    // back to the caller's numbering as a gather by the inverse: scattered reads cost
+    // less than scattered partial-sector writes when the numbering has no locality
+    std::vector<int32_t> inv((size_t)n);
+    for (long long i = 0; i < n; ++i) inv[(size_t)free_id[i]] = (int32_t)i;
     op->d_numbering = dalloc<int32_t>((size_t)n);
+    op->d_numbering_inv = dalloc<int32_t>((size_t)n);
     SF_CUDA_CHECK(cudaMemcpy(op->d_numbering, free_id, (size_t)n * sizeof(int32_t),
+                             cudaMemcpyHostToDevice));
+    SF_CUDA_CHECK(cudaMemcpy(op->d_numbering_inv, inv.data(), (size_t)n * sizeof(int32_t),
                              cudaMemcpyHostToDevice));
   });
 }
@@ -1168,7 +1178,7 @@ int sf_rhs(sf_op* op, const double* fq, double* b, void* stream) {
         LexScope lex(op);
         check_status(sf_rhs(op, fq, bl, stream), op);
       }
-      sf::permute_scatter(SF_F64, bl, op->d_numbering, b, op->n_free, st);
+      sf::permute_gather(SF_F64, bl, op->d_numbering_inv, b, op->n_free, st);
       return;
     }
     SF_CUDA_CHECK(cudaMemsetAsync(b, 0, op->n_free * sizeof(double), st));
@@ -1190,7 +1200,7 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream) {
         LexScope lex(op);
         check_status(sf_diagonal(op, dtype, dl, stream), op);
       }
-      sf::permute_scatter(dtype, dl, op->d_numbering, d, op->n_free, st);
+      sf::permute_gather(dtype, dl, op->d_numbering_inv, d, op->n_free, st);
       return;
     }
     if (op->slab || op->D == 2) {
@@ -1238,7 +1248,7 @@ int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int ma
       else
         it = cg_f64(op, mode == SF_CG_F64, bs, xs, reltol, maxiter, &rel, st);
     }
-    if (perm) sf::permute_scatter(SF_F64, xs, op->d_numbering, x, op->n_free, st);
+    if (perm) sf::permute_gather(SF_F64, xs, op->d_numbering_inv, x, op->n_free, st);
     op->last_inner = it;
     op->last_outer = outer;
     op->last_relres = rel;
