@@ -754,6 +754,8 @@ def run_table_gather(sf, dev, n=64, p=P, seed=7):
             byts = (ids_bytes if gather == "table" else 0) + ndof * 2 * vb
             out[key] = {"ms": round(ms, 3), "gdof_s": round(ndof / (ms * 1e-3) / 1e9, 2),
                         "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1)}
+        A.diagonal()
+        out["diagonal_ms"] = round(_events_ms(lambda: A.diagonal(), 3), 3)  # element form
         # FP64 Jacobi CG, 30 iterations (a numbered solve permutes b and x once)
         sf.cg(A, x, reltol=1e-300, maxiter=3, raise_on_fail=False)
         out["cg30_ms"] = round(_events_ms(lambda: sf.cg(A, x, reltol=1e-300, maxiter=30,

@@ -473,44 +473,117 @@ k_rhs(const __grid_constant__ GenParams<SB, SQ, double> P) {
 }
 
 // Diagonal of the assembled operator: for each cell and tensor position a,
-// diag_e[a] = sum_q sum_{r,s} G_rs(q) dphi_a/dxi_r(q) dphi_a/dxi_s(q), with the
-// 3D basis gradient a product of 1D values. One thread per (cell, a); the sum
-// over q is factorized into 1D sums when G is separable and diagonal, and
-// done point by point otherwise. Assembled with atomics (Jacobi needs diag(A)).
+//   diag_e[a] = sum_q kappa(q) sum_{r,s} G_rs(q) dphi_a/dxi_r(q) dphi_a/dxi_s(q).
+// The 3D gradient is a product of 1D values, so for each of the six symmetric
+// pairs (r, s) the product of two gradients is, direction by direction, one of
+// W0 = A*A, W1 = A*B, W2 = B*B (elementwise, [q][a]), and
+//   diag_e[a1 a2 a3] += c_rs sum_{q1 q2 q3} H_rs(q) W(q1,a1) W'(q2,a2) W''(q3,a3)
+// with H_rs = kappa G_rs and c_rs = 1 (r = s) or 2: three 1D contractions per pair
+// (sum factorization), about SB SQ^3 + SB^2 SQ^2 + SB^3 SQ multiply-adds each
+// instead of SB^3 SQ^3. One element per max(SB,SQ)^2 threads, as in k_general;
+// per element H, the two partial contractions and the diagonal sit in shared
+// memory. Assembled with atomics (Jacobi needs diag(A)).
+template <int SB, int SQ>
+struct DiagShape {
+  static constexpr int NQ = SQ * SQ * SQ;
+  static constexpr int WE = NQ + SB * SQ * SQ + SB * SB * SQ + SB * SB * SB;  // words per element
+};
+
 template <int SB, int SQ, typename T>
-__global__ void k_general_diag(const __grid_constant__ GenParams<SB, SQ, T> P) {
-  constexpr int S0 = SB * SB * SB;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.ncells * S0) return;
-  const long long cell = t / S0;
-  const int pos = (int)(t % S0);
-  long long id;
-  if (P.ids) id = P.ids[cell * S0 + pos];
-  else id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
-  if (id < 0) return;
-  const int a1 = pos % SB, a2 = (pos / SB) % SB, a3 = pos / (SB * SB);
-  double acc = 0.0;
-  for (int qk = 0; qk < SQ; ++qk)
-    for (int qj = 0; qj < SQ; ++qj)
-      for (int qi = 0; qi < SQ; ++qi) {
-        const int q = qi + SQ * (qj + SQ * qk);
-        const double Ax = (double)P.A[qi * SB + a1], Bx = (double)P.B[qi * SB + a1];
-        const double Ay = (double)P.A[qj * SB + a2], By = (double)P.B[qj * SB + a2];
-        const double Az = (double)P.A[qk * SB + a3], Bz = (double)P.B[qk * SB + a3];
-        const double gx = Bx * Ay * Az, gy = Ax * By * Az, gz = Ax * Ay * Bz;
-        double g[6];
+__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS)
+k_general_diag(const __grid_constant__ GenParams<SB, SQ, T> P) {
+  using S = Shape<SB, SQ>;
+  using DS = DiagShape<SB, SQ>;
+  constexpr int NQ = DS::NQ, S0 = SB * SB * SB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int el = threadIdx.x / S::NL;
+  const int l = threadIdx.x % S::NL;
+  const long long cell = (long long)blockIdx.x * S::EPB + el;
+  const bool valid = cell < P.ncells;
+  double* H = reinterpret_cast<double*>(smem_raw) + (size_t)el * DS::WE;  // [q3][q2][q1]
+  double* T1 = H + NQ;                // [q3][q2][a1]
+  double* T2 = T1 + SB * SQ * SQ;     // [q3][a2][a1]
+  double* D = T2 + SB * SB * SQ;      // [a3][a2][a1]
+  __shared__ double W[3][SQ * SB];    // A*A, A*B, B*B, [q][a]
+  for (int i = threadIdx.x; i < SQ * SB; i += S::THREADS) {
+    const double a = (double)P.A[i], b = (double)P.B[i];
+    W[0][i] = a * a;
+    W[1][i] = a * b;
+    W[2][i] = b * b;
+  }
+  for (int i = l; i < S0; i += S::NL) D[i] = 0.0;
+  const double* gt = P.gtab + (valid ? cell : 0) * P.gstride;
+#pragma unroll 1
+  for (int k = 0; k < 6; ++k) {  // G components xx, yy, zz, xy, xz, yz
+    const int r = k < 3 ? k : (k == 5 ? 1 : 0);
+    const int sp = k < 3 ? k : (k == 3 ? 1 : 2);
+    const double cf = k < 3 ? 1.0 : 2.0;
+    __syncthreads();  // W written; the last pass of the previous pair has read H
+    for (int q = l; q < NQ; q += S::NL) {
+      double g = 0.0;
+      if (valid) {
         if (P.geom == GEOM_SEPARABLE) {
-          const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
-          for (int c = 0; c < 6; ++c) g[c] = s * P.G0[c];
+          const int qi = q % SQ, qj = (q / SQ) % SQ, qk = q / (SQ * SQ);
+          g = P.w1[qi] * P.w1[qj] * P.w1[qk] * P.G0[k];
         } else {
-          const double* gt = P.gtab + cell * P.gstride;
-          for (int c = 0; c < 6; ++c) g[c] = gt[c * SQ * SQ * SQ + q];
+          g = gt[k * NQ + q];
         }
-        double kq = P.kappa ? P.kappa[cell * (SQ * SQ * SQ) + q] : 1.0;
-        acc += kq * (g[0] * gx * gx + g[1] * gy * gy + g[2] * gz * gz +
-                     2.0 * (g[3] * gx * gy + g[4] * gx * gz + g[5] * gy * gz));
+        if (P.kappa) g *= P.kappa[cell * NQ + q];
       }
-  atomicAdd(P.y + id, (T)acc);
+      H[q] = cf * g;
+    }
+    __syncthreads();
+    const double* W1 = W[(r == 0) + (sp == 0)];
+    const double* W2 = W[(r == 1) + (sp == 1)];
+    const double* W3 = W[(r == 2) + (sp == 2)];
+    if (l < SQ * SQ) {  // q1 -> a1 on lines (q2, q3)
+      double in[SQ];
+#pragma unroll
+      for (int q1 = 0; q1 < SQ; ++q1) in[q1] = H[l * SQ + q1];
+#pragma unroll
+      for (int a1 = 0; a1 < SB; ++a1) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q1 = 0; q1 < SQ; ++q1) acc = fma(W1[q1 * SB + a1], in[q1], acc);
+        T1[l * SB + a1] = acc;
+      }
+    }
+    __syncthreads();
+    if (l < SB * SQ) {  // q2 -> a2 on lines (a1, q3)
+      const int a1 = l % SB, q3 = l / SB;
+      double in[SQ];
+#pragma unroll
+      for (int q2 = 0; q2 < SQ; ++q2) in[q2] = T1[(q3 * SQ + q2) * SB + a1];
+#pragma unroll
+      for (int a2 = 0; a2 < SB; ++a2) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q2 = 0; q2 < SQ; ++q2) acc = fma(W2[q2 * SB + a2], in[q2], acc);
+        T2[(q3 * SB + a2) * SB + a1] = acc;
+      }
+    }
+    __syncthreads();
+    if (l < SB * SB) {  // q3 -> a3 on lines (a1, a2), added into the diagonal
+      double in[SQ];
+#pragma unroll
+      for (int q3 = 0; q3 < SQ; ++q3) in[q3] = T2[q3 * SB * SB + l];
+#pragma unroll
+      for (int a3 = 0; a3 < SB; ++a3) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q3 = 0; q3 < SQ; ++q3) acc = fma(W3[q3 * SB + a3], in[q3], acc);
+        D[a3 * SB * SB + l] += acc;
+      }
+    }
+  }
+  __syncthreads();
+  if (!valid) return;
+  for (int pos = l; pos < S0; pos += S::NL) {
+    long long id;
+    if (P.ids) id = P.ids[cell * S0 + pos];
+    else id = structured_index(cell, pos, SB, P.nx, P.ny, P.nz);
+    if (id >= 0) atomicAdd(P.y + id, (T)D[pos]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -743,10 +816,12 @@ void run_general(int mode, const double* A, const double* B, const Cells& cells,
   P.mode = mode;
   if (ncells == 0) return;
   if (mode == 2) {
-    const long long total = ncells * S::S0;
-    const int threads = 256;
-    const long long blocks = (total + threads - 1) / threads;
-    k_general_diag<SB, SQ, T><<<(unsigned)blocks, threads, 0, stream>>>(P);
+    const size_t smem = (size_t)S::EPB * DiagShape<SB, SQ>::WE * sizeof(double);
+    const long long blocks = (ncells + S::EPB - 1) / S::EPB;
+    SF_REQUIRE(blocks < (1LL << 31), SF_ERR_ARG, "too many cells for one launch");
+    SF_CUDA_CHECK(cudaFuncSetAttribute(k_general_diag<SB, SQ, T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_general_diag<SB, SQ, T><<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
     SF_CUDA_CHECK(cudaGetLastError());
     return;
   }

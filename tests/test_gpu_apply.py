@@ -221,3 +221,17 @@ def test_errors_are_reported(sf):
     x = torch.zeros(n, device="cuda", dtype=torch.float64)
     with pytest.raises(sf.SumFacError):
         sf.mul(x, A, x)  # aliasing is rejected by the library
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_diagonal_all_orders(sf, p):
+    """diag(A) (sum-factorized per element, assembled) against the assembled oracle, for
+    SQ below, at and above SB, on affine and on deformed cells."""
+    n = 2
+    for deg, pert in ((2 * p, 0.0), (max(2 * p - 2, 1), 0.0), (2 * p + 1, 0.15)):
+        A, V = build(sf, p, deg, n, pert, 4, "structured")
+        om = O.make_map(3, p, deg)
+        mesh = O.cartesian_mesh(3, n, p, om, perturb=pert, seed=4)
+        d_ref = O.assembled_sparse(om, mesh).diagonal()
+        d = A.diagonal().cpu().numpy()
+        assert relerr(d, d_ref) < TOL64, (p, deg, pert)
