@@ -104,8 +104,10 @@ int sf_set_structured(sf_op* op, int nx, int ny, int nz, const int32_t* node_ord
  * permutation of 0 .. n_free-1. This is the Cartesian mesh of the reference's
  * drivers with Gridap's own dof numbering (get_cell_dof_ids,
  * src/LazyMatrices.jl:46), which is not lexicographic. The tiled kernels still
- * run: sf_apply, sf_apply_multi and sf_mul_host permute x into lexicographic
- * order and the result back (two extra vector sweeps per apply); sf_cg permutes
+ * run: sf_apply, sf_apply_multi and sf_mul_host read x and write y through the
+ * numbering inside the kernel when it keeps neighbours near (option
+ * "numbered_fused"), else permute x into lexicographic order and the result
+ * back (two extra vector sweeps per apply); sf_cg permutes
  * b and x once per solve and iterates in lexicographic order; sf_diagonal and
  * sf_rhs compute lexicographically and permute the result. sf_kappa_vjp, the
  * sf_cgd_* steps, sf_cg_noalloc and the batched form reject such a handle.
@@ -265,6 +267,11 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *                          dropped by this factor (default 0.1)
  *   "tile_candidate_f64"  : force tile-shape candidate k of the tiled Cartesian kernel
  *   "tile_candidate_f32"    (0-based; see sf_get_info "tile_candidates_f64/f32")
+ *   "numbered_fused"      : after sf_set_structured_numbering, how an apply on the tiled
+ *                           kernel handles the numbering: 1 the kernel reads x and writes y
+ *                           through it; 0 x is permuted into lexicographic order and y back;
+ *                           -1 (default) 1 when most x-neighbours' ids lie within 64 of each
+ *                           other (a cell-by-cell numbering), else 0
  *   "jacobi_table"        : 1 (default): on a whole 3D Cartesian mesh the FP64 Jacobi CG's
  *                           vector kernels read D^-1 from a table per position in a cell
  *                           (it repeats cell to cell) instead of a vector; 0: from the vector
@@ -290,6 +297,7 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *                              unless the operator is a slab)
  *   "jacobi_table"           : 1 if sf_cg's FP64 Jacobi mode reads D^-1 from the table
  *   "numbered"               : 1 after sf_set_structured_numbering
+ *   "numbered_fused"         : 1 if applies read and write through the numbering in the kernel
  *   "cg_fused"               : 1 if sf_cg's FP64 modes use the fused CG kernel
  *   "cg_candidates"          : number of tile shapes of the fused CG kernel
  */

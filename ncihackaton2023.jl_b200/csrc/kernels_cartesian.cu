@@ -71,6 +71,7 @@ struct CartParams {
   int ntx, nty, ntz;  // tiles
   int tile0;          // first tile of the launch (CTA b applies tile tile0 + b)
   double* dot;  // non-null: dot[tile] = sum of x*y over the tile's outputs
+  const int32_t* num;  // numbered kernel: the vectors' index of each lexicographic free point
 };
 
 // FP64 sum over the CTA, valid in thread 0 (adds warps in a fixed order).
@@ -365,14 +366,17 @@ __device__ __forceinline__ void tile_passes(T* T1, T* T2, const EOMat<P, T>& Mm,
 // (p, A p) term of CG), summed in a fixed order. With PS non-null the z pass
 // keeps the x values of the owned points in PS (OX*OY*OZ shared words,
 // [zo][yo][xo]) for that sum, so they are not read from global memory a second
-// time; without it they are re-read.
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T>
+// time; without it they are re-read. NUM: x and y are in another numbering of
+// the free points, num[i] being the index of lexicographic point i; x is read
+// as x[num[i]] and y written as y[num[i]] (no (x, y) sum then).
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, bool NUM = false>
 __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
                                           const EOMat<P, T>& Km, const T* __restrict__ X,
                                           T* __restrict__ Y, int nfx, int nfy, int nfz, int zlo,
                                           int nfz_out, int tx,
                                           int ty, int tz, T rz, T rx, T cy,
-                                          double* dot = nullptr, T* PS = nullptr) {
+                                          double* dot = nullptr, T* PS = nullptr,
+                                          const int32_t* __restrict__ num = nullptr) {
   using G = Tile<P, EX, EY, EZ, T>;
   // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
   const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
@@ -385,7 +389,19 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
   auto load_col = [&](int l, T (&c)[G::BZ]) {
     const int x = l % G::BX, y = l / G::BX;
     const int fx = fx0 + x, fy = fy0 + y;
-    if (interior) {
+    if constexpr (NUM) {
+      const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
+      const long long ci = (long long)fx + (long long)nfx * fy;
+      int32_t k[G::BZ];
+#pragma unroll
+      for (int z = 0; z < G::BZ; ++z) {
+        const int fz = fz0 + z;
+        const bool in = interior || (inxy && (unsigned)(fz - zlo) < (unsigned)(nfz - zlo));
+        k[z] = in ? __ldg(num + ci + fz * pz) : -1;
+      }
+#pragma unroll
+      for (int z = 0; z < G::BZ; ++z) c[z] = k[z] >= 0 ? __ldg(X + k[z]) : T(0);
+    } else if (interior) {
       const T* col = X + (long long)fx + (long long)nfx * fy + fz0 * pz;
 #pragma unroll
       for (int z = 0; z < G::BZ; ++z) c[z] = __ldg(col + z * pz);
@@ -424,7 +440,10 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     for (int i = threadIdx.x; i < NOUT; i += NT) {
       long long o;
       int t1;
-      if (out_index(i, o, t1)) ybase[o] = T1[t1];
+      if (out_index(i, o, t1)) {
+        if constexpr (NUM) Y[__ldg(num + base + o)] = T1[t1];
+        else ybase[o] = T1[t1];
+      }
     }
     return;
   }
@@ -816,7 +835,7 @@ k_cartesian2d(const __grid_constant__ CartParams2<P, T> Q) {
 template <typename T>
 constexpr bool kStashDot = sizeof(T) == 4;
 
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB>
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB, bool NUM = false>
 __global__ void __launch_bounds__(NT, MINB)
 k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   using G = Tile<P, EX, EY, EZ, T>;
@@ -827,12 +846,12 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   Mm.load(Q.Me, Q.Mo);
   Km.load(Q.Ke, Q.Ko);
   const int tile = Q.tile0 + (int)blockIdx.x;
-  cart_tile<P, EX, EY, EZ, NT, ISO, T>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz, Q.zlo,
-                                       Q.nfz_out,
-                                       tile % Q.ntx, (tile / Q.ntx) % Q.nty,
-                                       tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy,
-                                       Q.dot ? Q.dot + tile : nullptr,
-                                       Q.dot && kStashDot<T> ? T2 + G::TS : nullptr);
+  cart_tile<P, EX, EY, EZ, NT, ISO, T, NUM>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz, Q.zlo,
+                                            Q.nfz_out,
+                                            tile % Q.ntx, (tile / Q.ntx) % Q.nty,
+                                            tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy,
+                                            Q.dot ? Q.dot + tile : nullptr,
+                                            Q.dot && kStashDot<T> ? T2 + G::TS : nullptr, Q.num);
 }
 
 // diag(A) on the free points written by an apply (full mesh or slab). On a
@@ -1005,6 +1024,9 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   Q.nty = (plan.ny + EY - 1) / EY;
   Q.ntz = (plan.nz + EZ - 1) / EZ;
   Q.dot = fuse.dot;
+  Q.num = fuse.num;
+  SF_REQUIRE(!fuse.num || (!fuse.dot && !plan.slab && fuse.tz1 < 0), SF_ERR_UNSUPPORTED,
+             "a numbered apply has no fused dot, slab or tile-row range");
   long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
   SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
   if (fuse.tz1 >= 0) {  // tile rows [tz0, tz1) only
@@ -1017,15 +1039,12 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   const size_t smem =
       ((size_t)G::WORDS + (fuse.dot && kStashDot<T> ? (size_t)G::OX * G::OY * G::OZ : 0)) *
       sizeof(T);
-  if (iso) {
-    auto kern = k_cartesian<P, EX, EY, EZ, NT, true, T, MINB>;
-    SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
-  } else {
-    auto kern = k_cartesian<P, EX, EY, EZ, NT, false, T, MINB>;
-    SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
-  }
+  auto kern = fuse.num ? (iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB, true>
+                              : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB, true>)
+                       : (iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB>
+                              : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB>);
+  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 

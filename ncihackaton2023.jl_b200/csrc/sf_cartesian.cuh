@@ -25,6 +25,9 @@ struct CartesianPlan {
 struct CartFuse {
   double* dot = nullptr;  // per-tile partial sums of x*y (cartesian_tiles entries)
   int tz0 = 0, tz1 = -1;  // tz1 >= 0: apply only the tile rows tz0 <= tz < tz1 (z-rows of tiles)
+  // x and y in another numbering of the free points: num[i] is the index of lexicographic
+  // point i (a whole mesh; no dot or tile-row range with it)
+  const int32_t* num = nullptr;
 };
 
 // Builds the 1D operators; returns false when no tiled kernel exists for SB.

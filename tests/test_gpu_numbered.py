@@ -27,9 +27,15 @@ def spaces(sf, p, n, seed=5):
     return m, model, A_num, A_tab, A_lex, perm
 
 
+@pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("p,n", [(2, (5, 4, 6)), (4, (4, 3, 5)), (3, (6, 6, 2))])
-def test_numbered_apply_matches_table(sf, p, n):
+def test_numbered_apply_matches_table(sf, p, n, fused):
+    """Both ways of applying through a numbering: permuting x and y around the
+    lexicographic apply (0), and the tiled kernel reading and writing through it (1)."""
     m, model, A_num, A_tab, A_lex, perm = spaces(sf, p, n)
+    assert A_num.info("numbered_fused") == 0.0  # a random numbering has no locality
+    A_num.set_option("numbered_fused", fused)
+    assert A_num.info("numbered_fused") == float(fused)
     assert A_num.uses_tiled_kernel() and not A_tab.uses_tiled_kernel()
     assert A_num.info("numbered") == 1.0 and A_tab.info("numbered") == 0.0
     x = torch.from_numpy(np.random.default_rng(p).uniform(-1, 1, A_num.n)).cuda()
@@ -121,6 +127,7 @@ def test_cellwise_numbering_matches_table(sf):
     m = sf.SumFactorizationMap(3, (4,) * 3, (8,) * 3)
     V = sf.FESpace(model, 4, cellwise=True)
     A_num = sf.LazyMatrix(m, V, V, sf.Measure(model, 8), gather="numbered")
+    assert A_num.info("numbered_fused") == 1.0  # a cell-by-cell numbering keeps neighbours near
     A_tab = sf.LazyMatrix(m, V, V, sf.Measure(model, 8), gather="table")
     x = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, A_num.n)).cuda()
     y_ref = A_tab @ x
