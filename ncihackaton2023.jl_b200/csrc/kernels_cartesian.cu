@@ -993,7 +993,8 @@ void run_batch(const CartesianPlan& proto, const void* d_probs, int nprob, long 
 }
 
 // One launch of the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
-template <int P, typename T, int EX, int EY, int EZ, int NT, int MINB>
+// NUM: x and y in the numbering fuse.num (the numbered kernel).
+template <int P, typename T, int EX, int EY, int EZ, int NT, int MINB, bool NUM = false>
 void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse& fuse,
               cudaStream_t st) {
   using G = Tile<P, EX, EY, EZ, T>;
@@ -1025,7 +1026,8 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   Q.ntz = (plan.nz + EZ - 1) / EZ;
   Q.dot = fuse.dot;
   Q.num = fuse.num;
-  SF_REQUIRE(!fuse.num || (!fuse.dot && !plan.slab && fuse.tz1 < 0), SF_ERR_UNSUPPORTED,
+  SF_REQUIRE(NUM == (fuse.num != nullptr), SF_ERR_STATE, "numbered kernel without a numbering");
+  SF_REQUIRE(!NUM || (!fuse.dot && !plan.slab && fuse.tz1 < 0), SF_ERR_UNSUPPORTED,
              "a numbered apply has no fused dot, slab or tile-row range");
   long long tiles = (long long)Q.ntx * Q.nty * Q.ntz;
   SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
@@ -1039,10 +1041,8 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   const size_t smem =
       ((size_t)G::WORDS + (fuse.dot && kStashDot<T> ? (size_t)G::OX * G::OY * G::OZ : 0)) *
       sizeof(T);
-  auto kern = fuse.num ? (iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB, true>
-                              : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB, true>)
-                       : (iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB>
-                              : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB>);
+  auto kern = iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB, NUM>
+                  : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB, NUM>;
   SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)tiles, NT, smem, st>>>(Q);
   SF_CUDA_CHECK(cudaGetLastError());
@@ -1130,13 +1130,12 @@ template <int P>
 struct CgCands;
 #define SF_CGC(P_, ...) \
   template <> struct CgCands<P_> { static constexpr CgCandidate c[] = {__VA_ARGS__}; };
-SF_CGC(1, SF_CGT(1, 8, 8, 4, 256, true, 2), SF_CGT(1, 8, 8, 4, 256, false, 2))
-SF_CGC(2, SF_CGT(2, 4, 4, 4, 256, true, 2), SF_CGT(2, 8, 4, 2, 256, false, 2))
-SF_CGC(3, SF_CGT(3, 4, 4, 2, 256, true, 2), SF_CGT(3, 4, 4, 2, 256, false, 3))
-SF_CGC(4, SF_CGT(4, 4, 4, 2, 256, false, 3), SF_CGT(4, 4, 4, 2, 256, true, 2),
-       SF_CGT(4, 4, 4, 2, 256, false, 2))
-SF_CGC(5, SF_CGT(5, 2, 2, 2, 256, false, 2), SF_CGT(5, 2, 2, 2, 256, true, 2))
-SF_CGC(6, SF_CGT(6, 2, 2, 2, 256, false, 1), SF_CGT(6, 2, 2, 1, 256, false, 2))
+SF_CGC(1, SF_CGT(1, 8, 8, 4, 256, true, 2))
+SF_CGC(2, SF_CGT(2, 4, 4, 4, 256, true, 2))
+SF_CGC(3, SF_CGT(3, 4, 4, 2, 256, true, 2))
+SF_CGC(4, SF_CGT(4, 4, 4, 2, 256, false, 3), SF_CGT(4, 4, 4, 2, 256, true, 2))
+SF_CGC(5, SF_CGT(5, 2, 2, 2, 256, false, 2))
+SF_CGC(6, SF_CGT(6, 2, 2, 2, 256, false, 1))
 SF_CGC(7, SF_CGT(7, 2, 2, 1, 256, false, 1))
 SF_CGC(8, SF_CGT(8, 2, 2, 1, 256, false, 1))
 #undef SF_CGC
@@ -1276,6 +1275,35 @@ SF_C2(8, SF_T2F(8, 8, 8, 2, 2, 256, 2))
 #undef SF_T2F
 #undef SF_TILE2
 
+// The numbered kernel: one tile shape per order and dtype (the autotuner's usual choice
+// on large meshes), which keeps its instantiations few.
+template <int P, typename T>
+struct NumTile;
+#define SF_NUMT(P_, T_, EX_, EY_, EZ_, NT_, MINB_)                           \
+  template <> struct NumTile<P_, T_> {                                      \
+    static constexpr RunFn run = &run_tile<P_, T_, EX_, EY_, EZ_, NT_, MINB_, true>; \
+  };
+SF_NUMT(1, double, 8, 8, 4, 256, 2) SF_NUMT(1, float, 8, 8, 4, 256, 2)
+SF_NUMT(2, double, 4, 4, 4, 256, 2) SF_NUMT(2, float, 4, 4, 4, 256, 2)
+SF_NUMT(3, double, 4, 4, 2, 256, 2) SF_NUMT(3, float, 4, 4, 4, 256, 2)
+SF_NUMT(4, double, 4, 4, 3, 256, 2) SF_NUMT(4, float, 4, 4, 3, 256, 4)
+SF_NUMT(5, double, 2, 2, 2, 256, 2) SF_NUMT(5, float, 2, 2, 2, 256, 2)
+SF_NUMT(6, double, 2, 2, 2, 256, 1) SF_NUMT(6, float, 2, 2, 2, 256, 2)
+SF_NUMT(7, double, 2, 2, 1, 256, 1) SF_NUMT(7, float, 2, 2, 2, 256, 2)
+SF_NUMT(8, double, 2, 2, 1, 256, 1) SF_NUMT(8, float, 2, 2, 1, 256, 2)
+#undef SF_NUMT
+
+template <typename T>
+RunFn numbered_run(int SB) {
+  switch (SB - 1) {
+#define SF_CASE(P_) \
+  case P_: return NumTile<P_, T>::run;
+    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
+#undef SF_CASE
+    default: throw Error(SF_ERR_UNSUPPORTED, "no tiled Cartesian kernel for this order");
+  }
+}
+
 template <typename T, int P>
 int cand_count() { return (int)(sizeof(Cands<P, T>::c) / sizeof(Candidate)); }
 
@@ -1400,6 +1428,12 @@ void cartesian_apply_candidate(const CartesianPlan& plan, int dtype, int k, cons
 void cartesian_apply(const CartesianPlan& plan, int dtype, const void* x, void* y,
                      cudaStream_t stream, const CartFuse& fuse) {
   SF_REQUIRE(plan.ready, SF_ERR_STATE, "Cartesian plan not prepared");
+  if (fuse.num) {  // the numbered kernel has its own tile shape
+    SF_REQUIRE(plan.D == 3, SF_ERR_UNSUPPORTED, "the numbered kernel is 3D");
+    (dtype_slot(dtype) == 0 ? numbered_run<double>(plan.SB) : numbered_run<float>(plan.SB))(
+        plan, x, y, fuse, stream);
+    return;
+  }
   pick(plan, dtype, plan.choice[dtype_slot(dtype)]).run(plan, x, y, fuse, stream);
 }
 
