@@ -42,8 +42,14 @@ def test_numbered_apply_matches_table(sf, p, n, fused):
     y_ref = A_tab @ x
     y = A_num @ x
     assert (y - y_ref).abs().max().item() <= 1e-12 * y_ref.abs().max().item()
-    # the same as the lexicographic operator on the permuted vector
-    assert torch.equal(y[perm], A_lex @ x[perm])
+    # the same as the lexicographic operator on the permuted vector: bit for bit through the
+    # permutation (the same kernel); to rounding in the numbered kernel, whose tile shape can
+    # differ (a vertex between tiles adds its cells' parts in another order)
+    y_lex = A_lex @ x[perm]
+    if fused:
+        assert (y[perm] - y_lex).abs().max().item() <= 1e-13 * y_lex.abs().max().item()
+    else:
+        assert torch.equal(y[perm], y_lex)
     y32 = A_num @ x.float()
     assert (y32.double() - y_ref).abs().max().item() <= 2e-5 * y_ref.abs().max().item()
     # host vectors (sf_mul_host)
