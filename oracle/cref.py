@@ -1,5 +1,5 @@
 """ctypes front end of oracle/libsumfac_ref.so, the C restatement of the
-reference CPU path (TEST INFRASTRUCTURE ONLY: the checker and the timed CPU
+reference CPU path (TEST INFRASTRUCTURE ONLY: the parity reference and the timed CPU
 baseline; see sumfac_ref.c)."""
 from __future__ import annotations
 

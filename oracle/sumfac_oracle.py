@@ -1,6 +1,6 @@
 """CPU oracle for the sum-factorized Laplacian apply (TEST INFRASTRUCTURE ONLY).
 
-This module is the checker. Only ``tests/``, ``__graft_entry__.smoke()`` and
+This module is the parity reference of the tests. Only ``tests/``, ``__graft_entry__.smoke()`` and
 the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import it.
 The product path (the CUDA library and its Python host layer) never calls it.
 

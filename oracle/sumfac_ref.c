@@ -1,6 +1,6 @@
 /*
  * sumfac_ref.c -- C restatement of the reference's CPU sum-factorization
- * path (TEST INFRASTRUCTURE ONLY: the checker and the timed CPU baseline).
+ * path (TEST INFRASTRUCTURE ONLY: the parity reference and the timed CPU baseline).
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU legs load the
  * shared object built from this file. The product never does.
