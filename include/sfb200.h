@@ -31,7 +31,7 @@ typedef struct sf_op sf_op;
 #define SF_ERR_ARG 1          /* invalid argument (sizes, null pointers, unsupported order) */
 #define SF_ERR_CUDA 2         /* a CUDA runtime call failed */
 #define SF_ERR_STATE 3        /* the handle is missing a required set-up step */
-#define SF_ERR_UNSUPPORTED 4  /* valid request that this build does not implement */
+#define SF_ERR_UNSUPPORTED 4  /* valid request that this library does not implement */
 #define SF_ERR_NOT_CONVERGED 5/* an iterative solve reached its iteration cap */
 #define SF_ERR_NONFINITE 6    /* NaN or Inf met in a solve */
 

@@ -58,7 +58,7 @@ class SumFactorizationMap:
         fe_orders = tuple(fe_orders)
         quad_orders = tuple(quad_orders)
         if D not in (2, 3):
-            raise NotImplementedError("this build implements D = 2 and D = 3")
+            raise NotImplementedError("this library implements D = 2 and D = 3")
         if len(set(fe_orders)) != 1 or len(set(quad_orders)) != 1:
             raise NotImplementedError("anisotropic orders are not supported (the reference's "
                                       "to_gpu(::SumFactorizationMap) is isotropic too)")
