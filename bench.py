@@ -68,6 +68,8 @@ def parse():
                     help="CG iteration budget of the deformed Q8 section (0: no CG)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the full-size parity checks against the C restatement")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the batched, adjoint, deformed-mesh, 2D and table-gather sections")
     ap.add_argument("--tile", type=int, default=None,
@@ -77,7 +79,8 @@ def parse():
     ap.add_argument("--cells", type=int, default=64,
                     help="cells per direction (64 is the benchmark; smaller only for profiling)")
     a = ap.parse_args()
-    global NCELL, N_DOF_TOTAL
+    global NCELL, N_DOF_TOTAL, DO_PARITY
+    DO_PARITY = not a.no_parity
     NCELL = a.cells
     N_DOF_TOTAL = (NCELL * P + 1) ** 3
     return a
@@ -179,6 +182,36 @@ def cpu_baseline_port(nsteps_full=3):
     return {"value": round(N_DOF_TOTAL / t / 1e9, 6), "unit": "GDOF/s", "cores": 1, "kind": "port",
             "sample": f"{nsteps_full} full Q4 64^3 applies after 1 warm-up, C restatement of the "
                       f"reference loops (oracle/sumfac_ref.c), 1 thread; {t:.3f} s per apply"}
+
+
+PARITY_TOL = {"f64": 1e-12, "f32": 2e-5}  # max |y - y_ref| / max |y_ref|, as in tests/
+
+
+def _relerr(y, y_ref):
+    return float(np.abs(y - y_ref).max() / max(np.abs(y_ref).max(), 1e-300))
+
+
+def parity_headline(sf, A, x0, y64, dev):
+    """Full-size parity of the benchmark apply, outside the timed region: the FP64
+    result of the timed loop (y64 = A x0) and an FP32 apply of x0 against the C
+    restatement of the reference loops (oracle/sumfac_ref.c, all host threads)."""
+    import torch
+    from oracle import cref
+    from oracle import sumfac_oracle as O
+    om = O.make_map(3, P, DEG)
+    mesh = O.cartesian_mesh(3, NCELL, P, om)
+    x = x0.cpu().numpy()
+    t0 = time.perf_counter()
+    y_ref = cref.mul_mesh(om, mesh, x)
+    t_ref = time.perf_counter() - t0
+    y32 = torch.empty(A.n, dtype=torch.float32, device=dev)
+    sf.mul(y32, A, x0.float())
+    e64 = _relerr(y64.cpu().numpy(), y_ref)
+    e32 = _relerr(y32.double().cpu().numpy(), y_ref)
+    return {"max_rel_err_f64": e64, "max_rel_err_f32": e32,
+            "pass": e64 <= PARITY_TOL["f64"] and e32 <= PARITY_TOL["f32"], "tol": PARITY_TOL,
+            "checker": f"C restatement of the reference loops, {cref.max_threads()} threads, "
+                       f"{t_ref:.2f} s", "x": "the timed loop's x (U[-1,1], seed 0)"}
 
 
 def time_tile_candidates(A, dev, reps=20):
@@ -360,6 +393,11 @@ def run_ours(args, rank, world, local_rank):
     ms_step = ms / args.steps
     value = world * N_DOF_TOTAL / (ms_step * 1e-3) / 1e9
     kernel_path = "tiled-cartesian" if A.uses_tiled_kernel() else "general-element"
+    parity = None
+    if rank == 0 and not args.no_parity:
+        log("parity of the benchmark apply")
+        parity = parity_headline(sf, A, xs[0], ys[0], dev)
+        log(f"parity: {parity}")
 
     # end to end through the public host-buffer call (mul! on host vectors)
     e2e = None
@@ -405,6 +443,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "4 rotating x/y pairs (1.09 GB) > 126 MB L2",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": e2e,
+        "parity": parity,
         "gpu_launches": args.steps * A.kernels_per_apply(),
         "roofline": roofline_entry(achieved, peaks,
                                    NCU_TRAFFIC_BYTES.get(kernel_path) if NCELL == 64 else None),
@@ -439,6 +478,7 @@ def run_ours(args, rank, world, local_rank):
 
 CG_MAXITER = 6000
 SECONDARY_BUDGET_S = 180.0
+DO_PARITY = True  # full-size parity checks of the secondary sections (--no-parity: off)
 
 
 def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER):
@@ -559,6 +599,10 @@ def run_batched(sf, dev, nprob=48, nrhs=4, seed=2024):
     dofs = sum((n * p + 1) ** 3 for n, p in specs) * nrhs
     out = {"problems": nprob, "nrhs": nrhs, "dof_total_x_rhs": dofs,
            "orders": sorted({p for _, p in specs})}
+    oracle_meshes = []
+    if DO_PARITY:
+        from oracle import cref
+        from oracle import sumfac_oracle as O
     for dt, key in ((torch.float64, "f64"), (torch.float32, "f32")):
         X, Y = [], []
         for i, op in enumerate(ops):
@@ -583,6 +627,25 @@ def run_batched(sf, dev, nprob=48, nrhs=4, seed=2024):
         out[key] = {"ms_graph": round(ms, 3), "gdof_s": round(dofs / (ms * 1e-3) / 1e9, 2),
                     "ms_one_problem_at_a_time": round(ms_seq, 3),
                     "speedup_vs_sequential": round(ms_seq / ms, 3), "group_tiles": tiles}
+        if DO_PARITY:
+            # every problem and right-hand side of the graph launch against the C
+            # restatement (the graph is run again so that Y is its result)
+            b.apply(X, Y)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            worst = 0.0
+            for i, (n, p) in enumerate(specs):
+                if len(oracle_meshes) <= i:
+                    om = O.make_map(3, p, 2 * p)
+                    oracle_meshes.append((om, O.cartesian_mesh(3, n, p, om)))
+                om, mesh = oracle_meshes[i]
+                xi, yi = X[i].double().cpu().numpy(), Y[i].double().cpu().numpy()
+                for j in range(nrhs):
+                    worst = max(worst, _relerr(yi[:, j], cref.mul_mesh(om, mesh, xi[:, j])))
+            out[key]["parity"] = {"max_rel_err": worst, "pass": worst <= PARITY_TOL[key],
+                                  "cases": f"{nprob} problems x {nrhs} right-hand sides",
+                                  "checker": f"C restatement, {cref.max_threads()} threads, "
+                                             f"{time.perf_counter() - t0:.1f} s"}
         del X, Y, b
         torch.cuda.empty_cache()
     return out
@@ -647,6 +710,7 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
            "setup_s": round(setup_s, 2), "kernel": A.kernel_name()}
     nq = (p + 1) ** 3
     gbytes = n ** 3 * nq * 6 * 8
+    ys_ = {}
     for dt, key, vb in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
         xx, yy = x.to(dt), y.to(dt)
         for _ in range(3):
@@ -655,6 +719,20 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
         byts = gbytes + (n * p + 1) ** 3 * 2 * vb
         res[key] = {"ms": round(ms, 3), "gdof_s": round((n * p + 1) ** 3 / (ms * 1e-3) / 1e9, 2),
                     "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1)}
+        ys_[key] = yy.double().cpu().numpy()
+    if DO_PARITY:  # the full-size applies against the C restatement (chunked geometry)
+        from oracle import cref
+        from oracle import sumfac_oracle as O
+        om = O.make_map(3, p, 2 * p)
+        mesh = O.cartesian_mesh(3, n, p, om, perturb=0.2, seed=seed)
+        t0 = time.perf_counter()
+        y_ref = cref.mul_mesh(om, mesh, x.cpu().numpy())
+        e = {k: _relerr(v, y_ref) for k, v in ys_.items()}
+        res["parity"] = {"max_rel_err_f64": e["f64"], "max_rel_err_f32": e["f32"],
+                         "pass": e["f64"] <= PARITY_TOL["f64"] and e["f32"] <= PARITY_TOL["f32"],
+                         "checker": f"C restatement, {cref.max_threads()} threads, "
+                                    f"{time.perf_counter() - t0:.1f} s"}
+        del mesh, y_ref
     b = torch.from_numpy(sf.assemble_rhs(m, V, lambda X: 3 * np.pi ** 2 *
                                          np.prod(np.sin(np.pi * X), axis=-1))).to(dev)
     log(f"deformed apply: {res}")

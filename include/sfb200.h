@@ -355,6 +355,14 @@ const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int group);
  * can cause. Same arguments and stopping rule as sf_cg. Modes SF_CG_F64 and
  * SF_CG_F64_PLAIN only (SF_CG_MIXED returns SF_ERR_UNSUPPORTED).
  *
+ * Operators it rejects although sf_cg takes them (SF_ERR_UNSUPPORTED): a
+ * Cartesian operator with the caller's dof numbering
+ * (sf_set_structured_numbering) and a slab operator (sf_set_structured_slab).
+ *
+ * The call reads the device's convergence flag once per 8 queued iterations
+ * and synchronises the stream to do so; it returns after the solve has
+ * finished on the device.
+ *
  * Limits and sharing:
  * - Its scratch is one static device array sized for n_free <= SF_NOALLOC_MAX_FREE
  *   (about 10 MB). Every GPU that loads the library holds it until exit.

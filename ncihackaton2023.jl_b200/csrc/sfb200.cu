@@ -1529,6 +1529,7 @@ namespace {
 
 constexpr long long kNoAllocMaxFree = SF_NOALLOC_MAX_FREE;
 constexpr long long kNoAllocScalarWords = 32;  // CG scalars, padded to 256 bytes
+constexpr int kNoAllocChunk = 8;               // iterations queued between reads of the flag
 constexpr long long kNoAllocWords =
     5 * kNoAllocMaxFree + kNoAllocScalarWords + 3LL * sf::kRedBlocks;
 static_assert((kNoAllocMaxFree * 8) % 256 == 0, "scratch vectors must stay 256-byte aligned");
@@ -1586,11 +1587,19 @@ int cg_f64_noalloc(sf_op* op, bool jacobi, const double* b, double* x, double re
   const double bb = read_scalar_noalloc(s, sf::CG_BB, st);
   const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
   double done = read_scalar_noalloc(s, sf::CG_DONE, st);
-  for (int it = 0; it < maxiter && done == 0.0; ++it) {
-    apply_impl(op, SF_F64, p, q, st);
-    sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, s, s + sf::CG_DONE, st);
-    sf::cg_update<double>(s, r, q, Dv, n, partials, st);
-    sf::cg_direction<double>(s, x, p, r, Dv, n, nullptr, st);
+  // Iterations are queued kNoAllocChunk at a time and the flag is read once per
+  // chunk. Every kernel of an iteration does nothing once the flag is set, so the
+  // iterations queued past convergence leave x, the residual and the count as
+  // they were.
+  for (int queued = 0; queued < maxiter && done == 0.0;) {
+    const int chunk = std::min(kNoAllocChunk, maxiter - queued);
+    for (int k = 0; k < chunk; ++k) {
+      apply_impl(op, SF_F64, p, q, st);
+      sf::vec_dot<double>(p, q, n, partials, s + sf::CG_PQ, s, s + sf::CG_DONE, st);
+      sf::cg_update<double>(s, r, q, Dv, n, partials, st);
+      sf::cg_direction<double>(s, x, p, r, Dv, n, nullptr, st);
+    }
+    queued += chunk;
     done = read_scalar_noalloc(s, sf::CG_DONE, st);
   }
   SF_REQUIRE(done != 3.0, SF_ERR_NONFINITE, "non-finite residual in CG");

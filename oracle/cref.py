@@ -103,3 +103,37 @@ def problem_from_oracle(m, mesh, cq, kappa=None, colors=True) -> Problem:
     col, ncol = cartesian_colors(mesh.n) if colors else (None, 0)
     return Problem(m.A0, m.B0, m.dof_map, mesh.cell_dof_ids, mesh.n_free, fill, wq, jq, djq, kappa,
                    col, ncol)
+
+
+def mul_mesh(m, mesh, x: np.ndarray, nthreads: int | None = None, layers: int = 4,
+             kappa: np.ndarray | None = None) -> np.ndarray:
+    """y = A x on a whole 3D oracle mesh by the C restatement, with all host
+    threads by default. An affine mesh without kappa passes its geometry as a
+    Fill. Otherwise the cells are taken in chunks of `layers` z-layers (an even
+    number, so the parity colouring of each chunk is valid), so that only one
+    chunk's per-point geometry is held on the host at a time, and the chunks'
+    contributions are added. This is the checker of the full-size parity runs."""
+    import copy
+
+    from oracle import sumfac_oracle as O
+    nthreads = max_threads() if nthreads is None else nthreads
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    if mesh.affine and kappa is None:
+        return problem_from_oracle(m, mesh, O.cell_quantities(m, mesh)).mul(x, nthreads=nthreads)
+    assert layers % 2 == 0 and mesh.D == 3
+    nx, ny, nz = mesh.n
+    per = nx * ny
+    y = np.zeros(mesh.n_free)
+    for z0 in range(0, nz, layers):
+        z1 = min(nz, z0 + layers)
+        cells = slice(z0 * per, z1 * per)
+        sub = copy.copy(mesh)
+        sub.n = (nx, ny, z1 - z0)
+        sub.cell_vertices = mesh.cell_vertices[cells]
+        sub.cell_dof_ids = mesh.cell_dof_ids[cells]
+        wq, jq, djq = (np.ascontiguousarray(a) for a in O.cell_quantities(m, sub))
+        col, ncol = cartesian_colors(sub.n)
+        prob = Problem(m.A0, m.B0, m.dof_map, sub.cell_dof_ids, mesh.n_free, False, wq, jq, djq,
+                       None if kappa is None else kappa[cells], col, ncol)
+        y += prob.mul(x, nthreads=nthreads)
+    return y

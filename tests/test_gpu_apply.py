@@ -93,6 +93,29 @@ def test_every_tile_candidate(sf, p, deg):
         assert relerr(y, y_ref) < tol, name
 
 
+@pytest.mark.parametrize("p,deg,n,perturb", [(4, 8, 24, 0.0), (2, 4, 40, 0.0), (8, 16, 6, 0.2),
+                                             (4, 8, 10, 0.2)])
+def test_midsize_against_c_restatement(sf, p, deg, n, perturb):
+    """Meshes of many tiles (Q4 on 24^3 cells: 6 x 6 x 8 tiles of the headline
+    kernel) and deformed meshes against the C restatement of the reference
+    loops, FP64 and FP32, with the default and the autotuned tile shape."""
+    from oracle import cref
+    torch = _torch()
+    A, V = build(sf, p, deg, n, perturb=perturb, seed=3)
+    om = O.make_map(3, p, deg)
+    mesh = O.cartesian_mesh(3, n, p, om, perturb=perturb, seed=3)
+    x = np.random.default_rng(n).uniform(-1, 1, mesh.n_free)
+    y_ref = cref.mul_mesh(om, mesh, x, layers=2)
+    xd = torch.from_numpy(x).cuda()
+    for dt, tol in ((torch.float64, TOL64), (torch.float32, TOL32)):
+        y = (A @ xd.to(dt)).double().cpu().numpy()
+        assert relerr(y, y_ref) < tol, (dt, A.kernel_name(dt))
+        if A.uses_tiled_kernel():
+            A.autotune(dt)
+            y = (A @ xd.to(dt)).double().cpu().numpy()
+            assert relerr(y, y_ref) < tol, (dt, A.kernel_name(dt))
+
+
 def test_renumbered_table(sf):
     torch = _torch()
     p, deg, n = 3, 6, 4

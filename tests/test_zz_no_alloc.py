@@ -49,9 +49,29 @@ def test_cg_noalloc_matches_cg(sf, mode, gather, p, deg, n):
         x = torch.zeros_like(b)
         st, it, rel = _cg_noalloc(A, code, b, x, 1e-10, A.n)
         assert st == _lib.SF_OK, _lib.lib.sf_last_error(A._h)
-        assert it == info["iters"] and rel <= 1e-10
+        # sf_cg may take (p, Ap) from per-tile sums and D^-1 from the Jacobi table,
+        # this entry point from a vector dot and the D^-1 vector: the rounding differs,
+        # so a residual near the tolerance may stop one iteration apart
+        assert abs(it - info["iters"]) <= 1 and rel <= 1e-10
         err = ((x - x_ref).abs().max() / x_ref.abs().max()).item()
         assert err < 1e-12
+
+
+def test_cg_noalloc_iteration_cap(sf):
+    """Iterations are queued several at a time: a cap that is not a multiple of
+    that chunk still stops the solve after exactly `maxiter` iterations."""
+    import torch
+    from ncihackaton2023_b200 import _lib
+    A, b_np = _problem(sf, 2, 4, 6, "structured")
+    b = torch.from_numpy(b_np).cuda()
+    x_ref, info = sf.cg(A, b, reltol=1e-300, maxiter=5, mode="jacobi", raise_on_fail=False)
+    assert info["iters"] == 5
+    x = torch.zeros_like(b)
+    st, it, rel = _cg_noalloc(A, _lib.SF_CG_F64, b, x, 1e-300, 5)
+    assert st == _lib.SF_ERR_NOT_CONVERGED and it == 5
+    assert rel > 0
+    err = ((x - x_ref).abs().max() / x_ref.abs().max()).item()
+    assert err < 1e-12
 
 
 def test_cg_noalloc_rejects_large_and_mixed(sf):
