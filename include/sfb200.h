@@ -345,6 +345,49 @@ int sf_batch_autotune(sf_batch* b, int dtype, const void* const* x, void* const*
 const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int group);
 
 /*
+ * Multigrid-preconditioned flexible CG on structured meshes. New: the
+ * reference solves with IterativeSolvers.cg! and no preconditioner
+ * (profiling/drivers.jl:85-95); this is the solver for the problems that CG
+ * cannot finish in reasonable time (equispaced high order on perturbed cells).
+ *
+ * sf_mg_create(out, A, nlevels, levels, transfer, basis_change)
+ *   A         the operator of the solve (its FP64 apply runs in the outer CG)
+ *   levels    nlevels operators, finest first, each a whole 3D structured mesh
+ *             (sf_set_structured, geometry set). Level l+1 has the cells of
+ *             level l (p-coarsening) or r times fewer per axis (h-coarsening),
+ *             and a space contained in level l's. levels[0] has A's mesh and order.
+ *   transfer  nlevels-1 row-major tables, transfer[l] of (r p_l + 1) x (p_{l+1} + 1)
+ *             doubles: entry [i][m] is coarse 1D basis function m of one coarse
+ *             cell at the i-th fine node of that cell (r fine cells of order p_l
+ *             along the axis, nodes in ascending position)
+ *   basis_change  NULL when levels[0] uses A's basis; else the (p+1) x (p+1)
+ *             row-major table [i][m] = levels[0]'s 1D basis function m at A's
+ *             i-th node (ascending positions): the hierarchy then works in
+ *             levels[0]'s basis and preconditions A through that change of basis.
+ * Set-up estimates the largest eigenvalue of D^-1 A on every level. On failure
+ * *out still receives a handle holding the message (sf_mg_last_error); destroy it.
+ * The handle borrows the operators: they must outlive it.
+ *
+ * sf_mg_cg: x (device, FP64, initial guess on entry) solves A x = b to
+ * ||b - A x|| <= reltol ||b||. mode SF_MG_MIXED runs the V-cycle in FP32 (outer
+ * CG, residual and dots in FP64), SF_MG_F64 all in FP64; one handle solves in
+ * one mode. Options (sf_mg_set_option): "degree" (Chebyshev smoothing steps, 2),
+ * "ratio" (smoothing range lmax/ratio..1.1 lmax, 30), "coarse_steps" (20),
+ * "coarse_ratio" (100). sf_mg_get_info: "levels", "lmax<l>", "n<l>", "graph".
+ */
+#define SF_MG_MIXED 0
+#define SF_MG_F64 1
+typedef struct sf_mg sf_mg;
+int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
+                 const double* const* transfer, const double* basis_change);
+int sf_mg_destroy(sf_mg* mg);
+const char* sf_mg_last_error(const sf_mg* mg);
+int sf_mg_set_option(sf_mg* mg, const char* name, double value);
+int sf_mg_get_info(const sf_mg* mg, const char* key, double* value);
+int sf_mg_cg(sf_mg* mg, int mode, const double* b, double* x, double reltol, int maxiter,
+             int* iters, double* relres, void* stream);
+
+/*
  * sf_cg_noalloc: sf_cg without any device or pinned-host allocation. It has no
  * counterpart in the reference.
  *

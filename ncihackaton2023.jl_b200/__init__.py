@@ -11,7 +11,8 @@ from . import fem
 from ._lib import LIB_PATH, SumFacError
 from .fem import (CartesianDiscreteModel, FESpace, Measure, Table, TrialFESpace,
                   cell_quantities)
-from . import adjoint, batch, distributed
+from . import adjoint, batch, distributed, multigrid
+from .multigrid import Multigrid
 from .operator import (LazyMatrix, SumFactorizationMap, assemble_rhs, cg, get_dimensional_parameters,
                        mul, mul_multi, quadrature_points, rhs)
 
@@ -19,5 +20,5 @@ __all__ = [
     "CartesianDiscreteModel", "FESpace", "TrialFESpace", "Measure", "Table", "cell_quantities",
     "SumFactorizationMap", "get_dimensional_parameters", "LazyMatrix", "mul", "mul_multi", "cg",
     "assemble_rhs", "rhs", "quadrature_points", "SumFacError", "LIB_PATH", "fem", "adjoint",
-    "batch", "distributed",
+    "batch", "distributed", "multigrid", "Multigrid",
 ]

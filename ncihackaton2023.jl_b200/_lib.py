@@ -33,6 +33,9 @@ SF_CG_F64 = 0
 SF_CG_MIXED = 1
 SF_CG_F64_PLAIN = 2
 
+SF_MG_MIXED = 0
+SF_MG_F64 = 1
+
 vp = C.c_void_p
 i32 = C.c_int
 i64 = C.c_int64
@@ -82,6 +85,12 @@ SIGNATURES = {
     "sf_cgd_apply": (i32, [vp, vp, vp, vp, vp]),
     "sf_cgd_update": (i32, [vp, vp, vp, vp, vp]),
     "sf_cgd_direction": (i32, [vp, vp, vp, vp, vp, vp]),
+    "sf_mg_create": (i32, [C.POINTER(vp), vp, i32, C.POINTER(vp), C.POINTER(vp), vp]),
+    "sf_mg_destroy": (i32, [vp]),
+    "sf_mg_last_error": (C.c_char_p, [vp]),
+    "sf_mg_set_option": (i32, [vp, C.c_char_p, C.c_double]),
+    "sf_mg_get_info": (i32, [vp, C.c_char_p, dp]),
+    "sf_mg_cg": (i32, [vp, i32, vp, vp, C.c_double, i32, C.POINTER(i32), dp, vp]),
 }
 
 SF_NOALLOC_MAX_FREE = 262144

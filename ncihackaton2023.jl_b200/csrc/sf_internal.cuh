@@ -78,4 +78,16 @@ void launch_general_evaluate(int dtype, int SB, int SQ, const double* A, const d
                              long long ncells, const int32_t* t2l, const Geometry& geom,
                              const void* x_cells, void* y_cells, cudaStream_t stream);
 
+// Access to an operator handle from other translation units (sfb200.cu).
+struct OpShape {
+  bool structured = false;  // whole 3D structured mesh, own numbering, geometry set
+  int nx = 0, ny = 0, nz = 0, p = 0;
+  long long n_free = 0;
+};
+OpShape op_shape(const sf_op* op);
+// y = A x (dtype SF_F64 / SF_F32) on the stream; throws Error on failure.
+void op_apply(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st);
+// FP64 diag(A) into d (n_free entries, written in full).
+void op_diag(sf_op* op, double* d, cudaStream_t st);
+
 }  // namespace sf

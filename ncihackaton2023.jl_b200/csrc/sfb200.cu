@@ -1931,3 +1931,31 @@ extern "C" const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int g
   return sf::cartesian_candidate_name(b->ops[grp.members[0]]->cart, dtype,
                                       grp.cand[dtype == SF_F64 ? 0 : 1]);
 }
+
+// ---------------------------------------------------------------------------
+// Operator access for the other translation units (the multigrid solver).
+// ---------------------------------------------------------------------------
+namespace sf {
+
+OpShape op_shape(const sf_op* op) {
+  OpShape s;
+  s.structured = op && op->cells.mesh == MESH_STRUCTURED && op->D == 3 && !op->slab &&
+                 !op->d_numbering && op->geom.kind != GEOM_NONE &&
+                 (op->cq_cells == 0 || op->cq_cells == op->cells.ncells);
+  if (!op) return s;
+  s.nx = op->cells.nx;
+  s.ny = op->cells.ny;
+  s.nz = op->cells.nz;
+  s.p = op->p;
+  s.n_free = op->n_free;
+  return s;
+}
+
+void op_apply(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
+  apply_impl(op, dtype, x, y, st);
+}
+
+void op_diag(sf_op* op, double* d, cudaStream_t st) { compute_diag(op, d, st); }
+
+
+}  // namespace sf

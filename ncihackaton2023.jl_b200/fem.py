@@ -40,6 +40,18 @@ def lagrange_nodes(p: int) -> np.ndarray:
     return np.array([0.0, 1.0] + [i / p for i in range(1, p)])
 
 
+def gll_nodes(p: int) -> np.ndarray:
+    """Gauss-Lobatto-Legendre nodes on [0, 1] in Gridap's SEGMENT order (vertex 0,
+    vertex 1, interior ascending): the end points and the roots of P_p'. The
+    multigrid hierarchy of an equispaced high-order space works in this basis."""
+    if p == 1:
+        return np.array([0.0, 1.0])
+    c = np.zeros(p + 1)
+    c[p] = 1.0
+    inner = np.sort(np.real(np.polynomial.legendre.legroots(np.polynomial.legendre.legder(c))))
+    return np.concatenate([[0.0, 1.0], 0.5 * (inner + 1.0)])
+
+
 def node_order(p: int) -> np.ndarray:
     """Position 0..p along the segment of each 1D basis function (Gridap order)."""
     return np.array([0, p] + list(range(1, p)), dtype=np.int32)
@@ -140,6 +152,19 @@ class CartesianDiscreteModel:
     @property
     def num_cells(self) -> int:
         return int(np.prod(self.partition))
+
+    def coarsened(self) -> "CartesianDiscreteModel":
+        """The model of every second vertex along each axis (half the cells; the
+        partition must be even): the coarse mesh of an h-multigrid level. On a
+        perturbed model its cells are the trilinear cells through those vertices."""
+        if self.D != 3 or any(n % 2 for n in self.partition):
+            raise ValueError("coarsening needs a 3D model with an even partition")
+        c = CartesianDiscreteModel(self.domain, tuple(n // 2 for n in self.partition))
+        nx, ny, nz = self.partition
+        v = self.vertices.reshape(nz + 1, ny + 1, nx + 1, 3)[::2, ::2, ::2]
+        c.vertices = np.ascontiguousarray(v.reshape(-1, 3))
+        c.perturb = self.perturb  # deformed cells stay deformed (per-cell geometry)
+        return c
 
     @property
     def is_affine_cartesian(self) -> bool:

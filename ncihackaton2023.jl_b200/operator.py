@@ -54,7 +54,7 @@ class SumFactorizationMap:
     gradMats[d][r] = (d != r) ? A0 : B0, and dof_map. quad_orders are
     quadrature DEGREES (Gridap convention: ceil((deg+1)/2) points)."""
 
-    def __init__(self, D: int, fe_orders, quad_orders):
+    def __init__(self, D: int, fe_orders, quad_orders, nodes: str = "equispaced"):
         fe_orders = tuple(fe_orders)
         quad_orders = tuple(quad_orders)
         if D not in (2, 3):
@@ -72,7 +72,13 @@ class SumFactorizationMap:
         self.SB = (p + 1,) * D
         self.SQ = (nq,) * D
         self.points, self.weights = fem.gauss_legendre(nq)
-        self.nodes = fem.lagrange_nodes(p)
+        # "equispaced": Gridap's Lagrangian nodes (the reference's map). "gll":
+        # Gauss-Lobatto nodes, the basis of the multigrid hierarchy of a
+        # high-order space (same space, better conditioned basis).
+        if nodes not in ("equispaced", "gll"):
+            raise ValueError("nodes must be 'equispaced' or 'gll'")
+        self.node_family = nodes
+        self.nodes = fem.lagrange_nodes(p) if nodes == "equispaced" else fem.gll_nodes(p)
         self.A0, self.B0 = fem.lagrange_basis(self.nodes, self.points)
         self.dof_map = fem.hex_dof_map(p, D)
         self.node_order = fem.node_order(p)
