@@ -90,3 +90,45 @@ def test_objective_gradient_fd_and_oracle(sf):
     Jm = objective(A, bd, uo, kd - eps * dd, reltol=1e-13)
     fd = (Jp - Jm) / (2 * eps)
     assert abs(fd - np.sum(g * d)) < 1e-5 * abs(fd)
+
+
+def test_rrule_call_sequence(sf):
+    """The C-ABI calls of the Julia ChainRulesCore.rrule binding: forward
+    sf_set_coefficient_device + sf_apply; pullback sf_apply(ybar) for x and
+    sf_kappa_vjp(x, ybar) for kappa. Checked against the torch autograd rule."""
+    import ctypes as C
+
+    import torch
+    from ncihackaton2023_b200 import _lib
+    from ncihackaton2023_b200.adjoint import kappa_apply
+    A, V, om, mesh = setup(sf, 3, 6, 3, 0.2, 4)
+    nc, nq = 27, 64
+    lib = _lib.lib
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(8)
+    kappa = torch.from_numpy(kappa_field(2, nc, nq)).cuda()
+    x = torch.from_numpy(rng.uniform(-1, 1, A.n)).cuda()
+    yb = torch.from_numpy(rng.uniform(-1, 1, A.n)).cuda()
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    # forward
+    assert lib.sf_set_coefficient_device(A._h, ptr(kappa), s) == _lib.SF_OK
+    y = torch.empty_like(x)
+    assert lib.sf_apply(A._h, _lib.SF_F64, ptr(x), ptr(y), s) == _lib.SF_OK
+    # pullback
+    assert lib.sf_set_coefficient_device(A._h, ptr(kappa), s) == _lib.SF_OK
+    xbar = torch.empty_like(x)
+    assert lib.sf_apply(A._h, _lib.SF_F64, ptr(yb), ptr(xbar), s) == _lib.SF_OK
+    kbar = torch.empty_like(kappa)
+    assert lib.sf_kappa_vjp(A._h, _lib.SF_F64, ptr(x), ptr(yb), ptr(kbar), s) == _lib.SF_OK
+    # the torch rule
+    xt = x.clone().requires_grad_(True)
+    kt = kappa.clone().requires_grad_(True)
+    yt = kappa_apply(A, xt, kt)
+    yt.backward(yb)
+    tol = lambda ref: 1e-12 * ref.abs().max().item()
+    assert (y - yt.detach()).abs().max().item() <= tol(yt.detach())
+    assert (xbar - xt.grad).abs().max().item() <= tol(xt.grad)
+    assert (kbar - kt.grad).abs().max().item() <= tol(kt.grad)
+    # and the kappa pullback against the oracle's VJP
+    kb_ref = O.kappa_vjp(om, mesh, x.cpu().numpy(), yb.cpu().numpy())
+    assert np.abs(kbar.cpu().numpy() - kb_ref).max() < 1e-12 * np.abs(kb_ref).max()
