@@ -872,11 +872,15 @@ def run_table_gather(sf, dev, n=64, p=P, seed=7):
     for numbering, rseed, gather in (("lexicographic", None, "table"), ("random", seed, "table"),
                                      ("random_numbered", seed, "numbered"),
                                      ("cellwise", "cellwise", "table"),
-                                     ("cellwise_numbered", "cellwise", "numbered")):
+                                     ("cellwise_numbered", "cellwise", "numbered"),
+                                     ("gridap", "gridap", "table"),
+                                     ("gridap_numbered", "gridap", "numbered")):
         # "numbered": the same numbering through sf_set_structured_numbering (the tiled
         # kernel on permuted vectors; no table). "cellwise": free dofs numbered cell by cell
         if rseed == "cellwise":
             V = sf.FESpace(model, p, cellwise=True)
+        elif rseed == "gridap":  # grouped by face dimension, as Gridap's conforming spaces
+            V = sf.FESpace(model, p, numbering="gridap")
         else:
             V = sf.FESpace(model, p, renumber_seed=rseed)
         A = sf.LazyMatrix(m, V, V, sf.Measure(model, DEG), gather=gather)
@@ -884,6 +888,8 @@ def run_table_gather(sf, dev, n=64, p=P, seed=7):
         x = torch.from_numpy(np.random.default_rng(seed).uniform(-1, 1, A.n)).to(dev)
         y = torch.empty_like(x)
         out = {"kernel": A.kernel_name()}
+        if gather == "numbered":
+            out["numbered_fused"] = A.info("numbered_fused")
         for dt, key, vb in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
             xx, yy = x.to(dt), y.to(dt)
             for _ in range(3):

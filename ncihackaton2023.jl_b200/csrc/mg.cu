@@ -53,9 +53,11 @@ constexpr int kMaxW = 256;           // 1D transfer table entries
 constexpr int kChunk = 4;            // iterations replayed between reads of the flag
 
 // Scalar slots of the outer FCG.
+// S_COUNTER is slot 9, where op_apply_dot's reductions keep their block counter.
 enum MgSlot {
   S_ZQ = 0, S_PR, S_PQ, S_RR, S_BB, S_TOL2, S_DONE, S_ITERS, S_FIRST, S_COUNTER, S_NSLOTS = 16
 };
+static_assert(S_COUNTER == 9, "the reduction counter slot of op_apply_dot");
 
 // ---------------------------------------------------------------------------
 // 1D transfer pass along one axis of a structured free-point grid.
@@ -69,7 +71,7 @@ enum MgSlot {
 // each fine point with the cell the prolongation assigns it to.
 // ---------------------------------------------------------------------------
 struct PassParams {
-  long long n0, n1, n2;  // output grid (x fastest)
+  int n0, n1, n2;        // output grid (x fastest); n1, n2 <= 65535 (grid dimensions)
   int axis;              // 0 x, 1 y, 2 z
   int n_in;              // input points along the axis
   int ncc, F, pc;
@@ -80,56 +82,57 @@ struct PassParams {
 template <typename T>
 __global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict__ in,
                        const T* __restrict__ in2, T* __restrict__ out) {
-  const long long n = Q.n0 * Q.n1 * Q.n2;
+  // one thread per output point: x from the block's x index, y and z from the grid
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i0 >= Q.n0) return;
+  const int i1 = blockIdx.y, i2 = blockIdx.z;
   const int W1 = Q.pc + 1;
-  for (long long i = (long long)blockIdx.x * kT + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kT) {
-    const long long i0 = i % Q.n0, r = i / Q.n0, i1 = r % Q.n1, i2 = r / Q.n1;
-    long long idx, base, stride;  // the axis index of the output, input base and stride
-    if (Q.axis == 0) {
-      idx = i0;
-      stride = 1;
-      base = (long long)Q.n_in * (i1 + Q.n1 * i2);
-    } else if (Q.axis == 1) {
-      idx = i1;
-      stride = Q.n0;
-      base = i0 + Q.n0 * (long long)Q.n_in * i2;
-    } else {
-      idx = i2;
-      stride = Q.n0 * Q.n1;
-      base = i0 + Q.n0 * i1;
+  int idx;
+  long long base, stride;  // the axis index of the output, input base and stride
+  if (Q.axis == 0) {
+    idx = i0;
+    stride = 1;
+    base = (long long)Q.n_in * (i1 + Q.n1 * (long long)i2);
+  } else if (Q.axis == 1) {
+    idx = i1;
+    stride = Q.n0;
+    base = i0 + Q.n0 * (long long)Q.n_in * i2;
+  } else {
+    idx = i2;
+    stride = Q.n0 * Q.n1;
+    base = i0 + Q.n0 * (long long)i1;
+  }
+  auto at = [&](int k) {  // input at axis index k (0-based free index)
+    const long long o = base + k * stride;
+    return Q.subtract ? (double)in[o] - (double)in2[o] : (double)in[o];
+  };
+  double acc = 0.0;
+  if (!Q.transpose) {
+    const int g = idx + 1;
+    const int c = min(g / Q.F, Q.ncc - 1);
+    const int l = g - c * Q.F;
+    const int top = Q.ncc * Q.pc;
+    for (int m = 0; m <= Q.pc; ++m) {
+      const int j = c * Q.pc + m;
+      const double w = Q.W[l * W1 + m];
+      if (j > 0 && j < top && w != 0.0) acc += w * at(j - 1);
     }
-    auto at = [&](long long k) {  // input at axis index k (0-based free index)
-      const long long o = base + k * stride;
-      return Q.subtract ? (double)in[o] - (double)in2[o] : (double)in[o];
-    };
-    double acc = 0.0;
-    if (!Q.transpose) {
-      const int g = (int)idx + 1;
+  } else {
+    const int gj = idx + 1;
+    const int clo = max(0, (gj + Q.pc - 1) / Q.pc - 1), chi = min(Q.ncc - 1, gj / Q.pc);
+    const int glo = max(1, clo * Q.F), ghi = min(Q.ncc * Q.F - 1, (chi + 1) * Q.F);
+    for (int g = glo; g <= ghi; ++g) {
       const int c = min(g / Q.F, Q.ncc - 1);
       const int l = g - c * Q.F;
-      const int top = Q.ncc * Q.pc;
-      for (int m = 0; m <= Q.pc; ++m) {
-        const int j = c * Q.pc + m;
-        const double w = Q.W[l * W1 + m];
-        if (j > 0 && j < top && w != 0.0) acc += w * at(j - 1);
-      }
-    } else {
-      const int gj = (int)idx + 1;
-      const int clo = max(0, (gj + Q.pc - 1) / Q.pc - 1), chi = min(Q.ncc - 1, gj / Q.pc);
-      const int glo = max(1, clo * Q.F), ghi = min(Q.ncc * Q.F - 1, (chi + 1) * Q.F);
-      for (int g = glo; g <= ghi; ++g) {
-        const int c = min(g / Q.F, Q.ncc - 1);
-        const int l = g - c * Q.F;
-        const int m = gj - c * Q.pc;
-        if (m < 0 || m > Q.pc) continue;
-        const double w = Q.W[l * W1 + m];
-        if (w != 0.0) acc += w * at(g - 1);
-      }
+      const int m = gj - c * Q.pc;
+      if (m < 0 || m > Q.pc) continue;
+      const double w = Q.W[l * W1 + m];
+      if (w != 0.0) acc += w * at(g - 1);
     }
-    if (Q.accumulate) out[i] = (T)((double)out[i] + acc);
-    else out[i] = (T)acc;
   }
+  const long long o = i0 + Q.n0 * (i1 + Q.n1 * (long long)i2);
+  if (Q.accumulate) out[o] = (T)((double)out[o] + acc);
+  else out[o] = (T)acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -274,17 +277,6 @@ __global__ void k_fcg_dir(const TZ* __restrict__ z, double* __restrict__ p,
   if (last_block<1>(v, partials, s) && threadIdx.x == 0) s[S_PR] = v[0];
 }
 
-// (p, q) after the apply.
-__global__ void k_fcg_pq(const double* __restrict__ p, const double* __restrict__ q, long long n,
-                         double* __restrict__ partials, double* __restrict__ s) {
-  if (s[S_DONE] != 0.0) return;
-  double v[1] = {0.0};
-  for (long long i = (long long)blockIdx.x * kT + threadIdx.x; i < n;
-       i += (long long)gridDim.x * kT)
-    v[0] = fma(p[i], q[i], v[0]);
-  if (last_block<1>(v, partials, s) && threadIdx.x == 0) s[S_PQ] = v[0];
-}
-
 // alpha = (p, r) / (p, q); x += alpha p; r -= alpha q; rl = r; (r, r) and the test.
 template <typename TL>
 __global__ void k_fcg_update(double* __restrict__ x, double* __restrict__ r,
@@ -398,9 +390,9 @@ struct sf_mg {
   std::vector<Transfer> tr;
   bool has_basis = false;
   Transfer basis;  // change of basis at level 0 (F = pc = p)
-  int degree = 2;
+  int degree = 3;
   double ratio = 30.0;
-  int coarse_steps = 20;
+  int coarse_steps = 10;
   double coarse_ratio = 100.0;
   int dtype = -1;  // type of the allocated cycle buffers
   bool ready = false;
@@ -476,9 +468,9 @@ void pass(const sf_mg::Transfer& t, int ncc, int axis, bool transpose, long long
           long long n1, long long n2, int n_in, const T* in, const T* in2, T* out, bool acc,
           cudaStream_t st) {
   sf::PassParams Q{};
-  Q.n0 = n0;
-  Q.n1 = n1;
-  Q.n2 = n2;
+  Q.n0 = (int)n0;
+  Q.n1 = (int)n1;
+  Q.n2 = (int)n2;
   Q.axis = axis;
   Q.n_in = n_in;
   Q.ncc = ncc;
@@ -488,9 +480,11 @@ void pass(const sf_mg::Transfer& t, int ncc, int axis, bool transpose, long long
   Q.accumulate = acc ? 1 : 0;
   Q.subtract = in2 ? 1 : 0;
   std::copy(t.W.begin(), t.W.end(), Q.W);
-  const long long n = n0 * n1 * n2;
-  if (n == 0) return;
-  sf::k_pass<T><<<sf::grid_of(n), sf::kT, 0, st>>>(Q, in, in2, out);
+  if (n0 <= 0 || n1 <= 0 || n2 <= 0) return;
+  SF_REQUIRE(n1 <= 65535 && n2 <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
+  const int bx = (int)std::min<long long>(256, (n0 + 31) / 32 * 32);
+  const dim3 grid((unsigned)((n0 + bx - 1) / bx), (unsigned)n1, (unsigned)n2);
+  sf::k_pass<T><<<grid, bx, 0, st>>>(Q, in, in2, out);
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
@@ -669,8 +663,8 @@ void fcg_iteration(sf_mg* mg, int dt, cudaStream_t st) {
   const int g = sf::grid_of(n);
   sf::k_fcg_zq<TL><<<g, sf::kT, 0, st>>>(z, mg->q, n, mg->partials, mg->s);
   sf::k_fcg_dir<TL><<<g, sf::kT, 0, st>>>(z, mg->p, mg->r, n, mg->partials, mg->s);
-  sf::op_apply(mg->A, SF_F64, mg->p, mg->q, st);
-  sf::k_fcg_pq<<<g, sf::kT, 0, st>>>(mg->p, mg->q, n, mg->partials, mg->s);
+  sf::op_apply_dot(mg->A, mg->p, mg->q, mg->partials, mg->s + sf::S_PQ, mg->s,
+                   mg->s + sf::S_DONE, st);  // q = A p and (p, q)
   sf::k_fcg_update<TL><<<g, sf::kT, 0, st>>>(mg->x, mg->r, mg->p, mg->q,
                                               static_cast<TL*>(mg->rl), n, mg->partials, mg->s);
   SF_CUDA_CHECK(cudaGetLastError());
@@ -776,7 +770,8 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
     SF_CUDA_CHECK(cudaEventCreateWithFlags(&mg->ev_in, cudaEventDisableTiming));
     SF_CUDA_CHECK(cudaEventCreateWithFlags(&mg->ev_out, cudaEventDisableTiming));
     mg->s = static_cast<double*>(mg_alloc(mg, sf::S_NSLOTS * sizeof(double)));
-    mg->partials = static_cast<double*>(mg_alloc(mg, 2 * sf::kMgBlocks * sizeof(double)));
+    mg->partials = static_cast<double*>(mg_alloc(
+        mg, std::max<long long>(2 * sf::kMgBlocks, sf::op_dot_partials(A)) * sizeof(double)));
     SF_CUDA_CHECK(cudaMemsetAsync(mg->s, 0, sf::S_NSLOTS * sizeof(double), mg->cs));
     SF_CUDA_CHECK(cudaMallocHost(&mg->h_s, sf::S_NSLOTS * sizeof(double)));
     mg->x = static_cast<double*>(mg_alloc(mg, mg->n * 8));

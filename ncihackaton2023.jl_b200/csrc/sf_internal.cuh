@@ -89,5 +89,11 @@ OpShape op_shape(const sf_op* op);
 void op_apply(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st);
 // FP64 diag(A) into d (n_free entries, written in full).
 void op_diag(sf_op* op, double* d, cudaStream_t st);
+// y = A x (FP64) and *out = (x, y), a fixed-order sum through `partials`
+// (op_dot_partials(op) entries); s[9] holds the reduction's block counter (zero
+// between calls). Nothing is summed while *skip != 0.
+void op_apply_dot(sf_op* op, const double* x, double* y, double* partials, double* out, double* s,
+                  const double* skip, cudaStream_t st);
+long long op_dot_partials(const sf_op* op);
 
 }  // namespace sf

@@ -1957,5 +1957,20 @@ void op_apply(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
 
 void op_diag(sf_op* op, double* d, cudaStream_t st) { compute_diag(op, d, st); }
 
+void op_apply_dot(sf_op* op, const double* x, double* y, double* partials, double* out, double* s,
+                  const double* skip, cudaStream_t st) {
+  if (tiled(op, SF_F64) && !op->d_numbering) {  // the apply's store phase forms the sums
+    sf::CartFuse fuse;
+    fuse.dot = partials;
+    sf::cartesian_apply(op->cart, SF_F64, x, y, st, fuse);
+    sf::dot_finish(partials, sf::cartesian_tiles(op->cart, SF_F64), out, skip, st);
+  } else {
+    apply_impl(op, SF_F64, x, y, st);
+    sf::vec_dot<double>(x, y, op->n_free, partials, out, s, skip, st);
+  }
+}
+
+long long op_dot_partials(const sf_op* op) { return cg_partials(op); }
+
 
 }  // namespace sf

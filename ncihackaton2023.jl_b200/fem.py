@@ -190,6 +190,102 @@ class CartesianDiscreteModel:
         return out
 
 
+# Local edges and faces of a hexahedron as Gridap's HEX polytope lists them (vertices x
+# fastest): edges along x, then y, then z; faces z = 0, z = 1, y = 0, y = 1, x = 0, x = 1.
+# Each entry: (axis of the edge / normal axis of the face, offset of its lowest vertex).
+_HEX_EDGES = [(0, (0, 0, 0)), (0, (0, 1, 0)), (0, (0, 0, 1)), (0, (0, 1, 1)),
+              (1, (0, 0, 0)), (1, (1, 0, 0)), (1, (0, 0, 1)), (1, (1, 0, 1)),
+              (2, (0, 0, 0)), (2, (1, 0, 0)), (2, (0, 1, 0)), (2, (1, 1, 0))]
+_HEX_FACES = [(2, (0, 0, 0)), (2, (0, 0, 1)), (1, (0, 0, 0)), (1, (0, 1, 0)),
+              (0, (0, 0, 0)), (0, (1, 0, 0))]
+
+
+def gridap_free_numbering(model: "CartesianDiscreteModel", p: int) -> np.ndarray:
+    """Free-dof numbering of a conforming Q_p space as Gridap builds it, face
+    dimension by face dimension: the dofs owned by vertices (in vertex order),
+    then by edges, by faces, and the cell-interior dofs (cell by cell); the
+    Dirichlet dofs are left out and the free ones keep that order. Edges and
+    faces carry the numbers of the grid topology, which gives each a number when
+    it is first met going through the cells in order and through each cell's
+    local edges / faces in the HEX order. A face's own dofs run x fastest, an
+    edge's along its axis.
+
+    Restated from the conforming-space construction of Gridap (FESpaces,
+    ``_generate_face_to_own_dofs``; Geometry, the topology's face numbering). The
+    reference does not pin Gridap's version and Gridap does not run here, so this
+    numbering is UNPINNED: it has Gridap's structure (grouped by face dimension),
+    not a verified bit-for-bit copy. Returns perm with perm[i] = the 0-based id of
+    lexicographic free point i (the ``FESpace.perm`` convention)."""
+    if model.D != 3:
+        raise NotImplementedError("3D models only")
+    n = np.array(model.partition)
+    N = n * p
+    V = n + 1                                   # vertices per axis
+    vlin = lambda v: v[..., 0] + V[0] * (v[..., 1] + V[1] * v[..., 2])
+    nc = int(np.prod(n))
+    c = np.arange(nc)
+    cell = np.stack([c % n[0], (c // n[0]) % n[1], c // (n[0] * n[1])], axis=1)
+
+    def first_visit(table):
+        """Topology numbers of the entities of `table`: key of each (cell, local)."""
+        keys = np.stack([a * (int(np.prod(V)) + 1) + vlin(cell + np.array(off))
+                         for a, off in table], axis=1).ravel()
+        uniq, first = np.unique(keys, return_index=True)
+        order = np.argsort(first, kind="stable")  # entity number -> index into uniq
+        rank = np.empty(len(uniq), dtype=np.int64)
+        rank[order] = np.arange(len(uniq))
+        return uniq, rank                        # uniq sorted; rank[k] = number of uniq[k]
+
+    # free grid points, lexicographic (x fastest)
+    fz, fy, fx = np.meshgrid(*[np.arange(1, N[a]) for a in (2, 1, 0)], indexing="ij")
+    g = np.stack([fx.ravel(), fy.ravel(), fz.ravel()], axis=1)
+    aligned = (g % p) == 0
+    dim = 3 - aligned.sum(axis=1)
+    perm = np.empty(len(g), dtype=np.int64)
+    base = 0
+    # vertices: interior vertices in vertex order
+    m = dim == 0
+    vid = vlin(g[m] // p)
+    iv = np.unique(vid)
+    perm[m] = base + np.searchsorted(iv, vid)
+    base += len(iv)
+    # edges and faces: entities in topology order, own dofs in a fixed local order
+    for d, table in ((1, _HEX_EDGES), (2, _HEX_FACES)):
+        m = dim == d
+        gd = g[m]
+        al = aligned[m]
+        if d == 1:
+            axis = np.argmax(~al, axis=1)                # the edge's axis
+        else:
+            axis = np.argmax(al, axis=1)                 # the face's normal axis
+        low = gd // p                                    # lowest vertex of the entity
+        key = axis * (int(np.prod(V)) + 1) + vlin(low)
+        uniq, rank = first_visit(table)
+        number = rank[np.searchsorted(uniq, key)]
+        loc = gd % p - 1                                 # 0 .. p-2 on the free axes
+        if d == 1:
+            local = loc[np.arange(len(gd)), axis]
+            own = p - 1
+        else:
+            a1 = np.where(axis == 0, 1, 0)
+            a2 = np.where(axis == 2, 1, 2)
+            local = loc[np.arange(len(gd)), a1] + (p - 1) * loc[np.arange(len(gd)), a2]
+            own = (p - 1) ** 2
+        # entities with free dofs, in topology order, get consecutive blocks
+        used = np.unique(number)
+        perm[m] = base + np.searchsorted(used, number) * own + local
+        base += len(used) * own
+    # cell interiors: cells in order
+    m = dim == 3
+    gd = g[m]
+    cidx = gd // p
+    cid = cidx[:, 0] + n[0] * (cidx[:, 1] + n[1] * cidx[:, 2])
+    loc = gd % p - 1
+    own = (p - 1) ** 3
+    perm[m] = base + cid * own + loc[:, 0] + (p - 1) * (loc[:, 1] + (p - 1) * loc[:, 2])
+    return perm
+
+
 @dataclass
 class Table:
     """Gridap's ``Table``: CSR with 1-based ``ptrs`` (length n+1) into ``data``."""
@@ -214,13 +310,16 @@ class FESpace:
     locality). ``cellwise`` numbers the free dofs instead in the order in which
     they first appear going through the cells in order, each cell in its local
     dof order: a cell-by-cell numbering such as a finite-element library gives
-    its spaces (locality kept)."""
+    its spaces (locality kept). ``numbering="gridap"`` numbers the free dofs
+    grouped by face dimension, as Gridap's conforming spaces do
+    (``gridap_free_numbering``)."""
 
     model: CartesianDiscreteModel
     order: int
     dirichlet_tags: str = "boundary"
     renumber_seed: int | None = None
     cellwise: bool = False
+    numbering: str = "lexicographic"
 
     def __post_init__(self):
         if self.dirichlet_tags != "boundary":
@@ -232,6 +331,13 @@ class FESpace:
         self.perm = None
         if self.renumber_seed is not None and self.cellwise:
             raise ValueError("renumber_seed and cellwise are exclusive")
+        if self.numbering not in ("lexicographic", "gridap"):
+            raise ValueError("numbering must be 'lexicographic' or 'gridap'")
+        if self.numbering == "gridap":
+            if self.renumber_seed is not None or self.cellwise:
+                raise ValueError("numbering='gridap' excludes renumber_seed and cellwise")
+            self.perm = gridap_free_numbering(self.model, p)
+            return
         if self.renumber_seed is not None:
             self.perm = (np.random.default_rng(self.renumber_seed)
                          .permutation(self.num_free_dofs).astype(np.int64))

@@ -63,12 +63,13 @@ class Multigrid:
     mode: "mixed" (FP32 V-cycle, FP64 outer CG) or "f64". basis: "gll",
     "equispaced" or "auto" (GLL from order 5 up). degree: Chebyshev smoothing
     steps per pre- and post-smoothing. h_levels: add Q1 levels on coarser
-    meshes (default True). coarse_steps: Chebyshev steps on the coarsest level.
+    meshes (default True) while every axis keeps at least ``min_cells`` cells.
+    coarse_steps: Chebyshev steps on the coarsest level.
     """
 
-    def __init__(self, A: LazyMatrix, mode: str = "mixed", basis: str = "auto", degree: int = 2,
-                 ratio: float = 30.0, h_levels: bool = True, coarse_steps: int | None = None,
-                 min_cells: int = 2):
+    def __init__(self, A: LazyMatrix, mode: str = "mixed", basis: str = "auto", degree: int = 3,
+                 ratio: float = 30.0, h_levels: bool = True, coarse_steps: int = 10,
+                 min_cells: int = 8):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         if A.gather != "structured" or A.m.D != 3:
@@ -103,7 +104,9 @@ class Multigrid:
                 continue
             m = SumFactorizationMap(3, (q,) * 3, (2 * q,) * 3, nodes=fam)
             V = fem.FESpace(mdl, q)
-            self.levels.append(LazyMatrix(m, V, V, fem.Measure(mdl, 2 * q)))
+            same = l == 0 and m.quad_degree == A.m.quad_degree  # A's geometry, reused
+            self.levels.append(LazyMatrix(m, V, V, fem.Measure(mdl, 2 * q),
+                                          cell_quantities=A.cell_quantities if same else None))
         self.orders = [q for _, q, _ in levels]
         self.cells = [tuple(mdl.partition) for mdl, _, _ in levels]
         tables = []
@@ -128,8 +131,6 @@ class Multigrid:
             raise _lib.SumFacError(st, f"sf_mg_create: {msg}")
         self.set_option("degree", degree)
         self.set_option("ratio", ratio)
-        if coarse_steps is None:
-            coarse_steps = 20
         self.set_option("coarse_steps", coarse_steps)
 
     def close(self):

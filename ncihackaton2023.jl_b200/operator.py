@@ -115,7 +115,7 @@ class LazyMatrix:
     each apply, and once per solve in cg (sf_set_structured_numbering)."""
 
     def __init__(self, m: SumFactorizationMap, trial: fem.FESpace, test: fem.FESpace,
-                 dOmega: fem.Measure, gather: str = "structured"):
+                 dOmega: fem.Measure, gather: str = "structured", cell_quantities=None):
         if trial is not test:
             raise NotImplementedError("trial and test spaces must be the same space")
         if dOmega.degree != m.quad_degree:
@@ -154,7 +154,10 @@ class LazyMatrix:
                       "sf_set_cells")
             else:
                 raise ValueError("gather must be 'structured', 'table' or 'numbered'")
-            fill, wq, jq, djq = fem.cell_quantities(self.model, m.points, m.weights)
+            # cell_quantities: (fill, wq, jq, djq) of another operator on the same model
+            # and quadrature (the geometry does not depend on the basis), else computed here
+            fill, wq, jq, djq = (cell_quantities if cell_quantities is not None else
+                                 fem.cell_quantities(self.model, m.points, m.weights))
             self.cell_quantities = (fill, wq, jq, djq)
             wq, jq, djq = _f64(wq), _f64(jq), _f64(djq)
             check(lib.sf_set_cell_quantities(self._h, 1 if fill else 0, _ptr(wq), _ptr(jq), _ptr(djq)),

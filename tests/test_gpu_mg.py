@@ -39,8 +39,8 @@ def test_mg_cartesian_q4(sf, mode, rough):
     A, om, mesh = _setup(sf, 4, 8)
     b = (np.random.default_rng(1).uniform(-1, 1, mesh.n_free) if rough
          else O.rhs(om, mesh, O.sin_forcing))
-    mg = sf.Multigrid(A, mode=mode)
-    assert mg.orders == [4, 2, 1, 1, 1] and mg.cells[-1] == (2, 2, 2)
+    mg = sf.Multigrid(A, mode=mode, min_cells=4)
+    assert mg.orders == [4, 2, 1, 1] and mg.cells[-1] == (4, 4, 4)
     x, info = mg.solve(torch.from_numpy(b).cuda(), reltol=1e-10)
     assert info["converged"] and info["relres"] <= 1e-10
     assert info["iters"] <= 25, info  # Jacobi CG: 28 (smooth) / 317 (rough) here
@@ -71,8 +71,8 @@ def test_mg_deformed_h_levels(sf):
     import torch
     A, om, mesh = _setup(sf, 2, 8, perturb=0.2, seed=2)
     b = np.random.default_rng(3).uniform(-1, 1, mesh.n_free)
-    mg = sf.Multigrid(A, mode="mixed")
-    assert mg.cells == [(8, 8, 8), (8, 8, 8), (4, 4, 4), (2, 2, 2)]
+    mg = sf.Multigrid(A, mode="mixed", min_cells=4, degree=2)
+    assert mg.cells == [(8, 8, 8), (8, 8, 8), (4, 4, 4)]
     x, info = mg.solve(torch.from_numpy(b).cuda(), reltol=1e-10, maxiter=200)
     assert info["converged"] and info["iters"] <= 40, info
     _check_solution(om, mesh, b, x.cpu().numpy(), 1e-7)

@@ -138,3 +138,32 @@ def test_cellwise_numbering_matches_table(sf):
     x = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, A_num.n)).cuda()
     y_ref = A_tab @ x
     assert ((A_num @ x) - y_ref).abs().max().item() <= 1e-12 * y_ref.abs().max().item()
+
+
+@pytest.mark.parametrize("fused", [0, 1])
+@pytest.mark.parametrize("p,n", [(4, (4, 3, 5)), (2, (6, 5, 4)), (3, (3, 4, 3))])
+def test_gridap_numbering(sf, p, n, fused):
+    """The face-grouped numbering of a conforming space (vertex, edge, face and
+    interior dofs in turn) through the numbered tiled path: the apply against the
+    table path and the solve against the lexicographic one."""
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), n)
+    m = sf.SumFactorizationMap(3, (p,) * 3, (2 * p,) * 3)
+    dO = sf.Measure(model, 2 * p)
+    Vg = sf.FESpace(model, p, numbering="gridap")
+    Vl = sf.FESpace(model, p)
+    A_num = sf.LazyMatrix(m, Vg, Vg, dO, gather="numbered")
+    A_tab = sf.LazyMatrix(m, Vg, Vg, dO, gather="table")
+    A_lex = sf.LazyMatrix(m, Vl, Vl, dO)
+    A_num.set_option("numbered_fused", fused)
+    perm = torch.from_numpy(Vg.perm).cuda()
+    x = torch.from_numpy(np.random.default_rng(p).uniform(-1, 1, A_num.n)).cuda()
+    y_ref = A_tab @ x
+    y = A_num @ x
+    assert (y - y_ref).abs().max().item() <= 1e-12 * y_ref.abs().max().item()
+    y32 = A_num @ x.float()
+    assert (y32.double() - y_ref).abs().max().item() <= 2e-5 * y_ref.abs().max().item()
+    b = x
+    xs, info = sf.cg(A_num, b, reltol=1e-10)
+    xl, infol = sf.cg(A_lex, b[perm], reltol=1e-10)
+    assert info["iters"] == infol["iters"]
+    assert (xs[perm] - xl).abs().max().item() <= 1e-12 * xl.abs().max().item()

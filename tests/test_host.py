@@ -102,3 +102,32 @@ def test_cellwise_numbering(sf):
     assert np.array_equal(first, np.arange(1, first.size + 1))
     with pytest.raises(ValueError):
         sf.FESpace(model, 3, cellwise=True, renumber_seed=1)
+
+
+def test_gridap_numbering_groups_by_face_dimension(sf):
+    """Free dofs of the face-grouped numbering: a permutation; vertex dofs first in
+    vertex order, then edge, face and cell-interior dofs; each cell's interior dofs
+    consecutive (x fastest)."""
+    import numpy as np
+    p, n = 3, (3, 4, 2)
+    model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), n)
+    V = sf.FESpace(model, p, numbering="gridap")
+    perm = V.perm
+    nf = V.num_free_dofs
+    assert np.array_equal(np.sort(perm), np.arange(nf))
+    fx, fy, fz = V.free_grid
+    gz, gy, gx = np.meshgrid(np.arange(1, fz + 1), np.arange(1, fy + 1), np.arange(1, fx + 1),
+                             indexing="ij")
+    g = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1)
+    dim = 3 - ((g % p) == 0).sum(axis=1)
+    starts = [perm[dim == d].min() for d in range(4)]
+    ends = [perm[dim == d].max() for d in range(4)]
+    for d in range(3):  # the groups follow each other
+        assert ends[d] + 1 == starts[d + 1]
+    assert starts[0] == 0 and ends[3] == nf - 1
+    v = g[dim == 0] // p  # vertex dofs in vertex order (x fastest)
+    vl = v[:, 0] + (n[0] + 1) * (v[:, 1] + (n[1] + 1) * v[:, 2])
+    assert np.array_equal(np.argsort(perm[dim == 0]), np.argsort(vl, kind="stable"))
+    c = g[dim == 3] // p  # cell c's interior dofs: a block of (p-1)^3 ids
+    cid = c[:, 0] + n[0] * (c[:, 1] + n[1] * c[:, 2])
+    assert np.array_equal((perm[dim == 3] - starts[3]) // (p - 1) ** 3, cid)
