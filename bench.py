@@ -631,7 +631,9 @@ def run_batched(sf, dev, nprob=48, nrhs=4, seed=2024):
         ops.append(sf.LazyMatrix(m, V, V, sf.Measure(model, 2 * p)))
     dofs = sum((n * p + 1) ** 3 for n, p in specs) * nrhs
     out = {"problems": nprob, "nrhs": nrhs, "dof_total_x_rhs": dofs,
-           "orders": sorted({p for _, p in specs})}
+           "orders": sorted({p for _, p in specs}),
+           "launch": "one CUDA graph launch per apply: one persistent kernel per order group "
+                     "(problems of one order share it), the groups as concurrent graph branches"}
     oracle_meshes = []
     if DO_PARITY:
         from oracle import cref
@@ -657,9 +659,12 @@ def run_batched(sf, dev, nprob=48, nrhs=4, seed=2024):
                 sf.mul_multi(y, op, x)
         seq()
         ms_seq = _events_ms(seq, 3)
+        vb = 8 if key == "f64" else 4
+        alg = dofs * 2 * vb  # every right-hand side read and its result written once
         out[key] = {"ms_graph": round(ms, 3), "gdof_s": round(dofs / (ms * 1e-3) / 1e9, 2),
                     "ms_one_problem_at_a_time": round(ms_seq, 3),
-                    "speedup_vs_sequential": round(ms_seq / ms, 3), "group_tiles": tiles}
+                    "speedup_vs_sequential": round(ms_seq / ms, 3), "group_tiles": tiles,
+                    "alg_bytes": alg, "achieved_gbs": round(alg / (ms * 1e-3) / 1e9, 1)}
         if DO_PARITY:
             # every problem and right-hand side of the graph launch against the C
             # restatement (the graph is run again so that Y is its result)
