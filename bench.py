@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--cg-only", action="store_true",
                     help="only the CG solves (autotuned tiles; no apply leg): for profiling")
     ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
-    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d", "cg_fused",
+    ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d",
                                           "table_gather"],
                     default=None,
                     help="run only this secondary configuration (no apply leg): for profiling")
@@ -74,8 +74,6 @@ def parse():
                     help="skip the batched, adjoint, deformed-mesh, 2D and table-gather sections")
     ap.add_argument("--tile", type=int, default=None,
                     help="force tile candidate K of the FP64 tiled kernel (skips the autotuner)")
-    ap.add_argument("--cg-candidate", type=int, default=None,
-                    help="cg_fused section: only tile shape K of the fused CG kernel")
     ap.add_argument("--cells", type=int, default=64,
                     help="cells per direction (64 is the benchmark; smaller only for profiling)")
     a = ap.parse_args()
@@ -328,7 +326,61 @@ def run_slabs(args, sf, rank, world, dev):
         "clocks": clk.summary(),
     }
     out["roofline"]["algorithmic_bytes_per_launch"] = alg_bytes
+    try:
+        out["batched_sharded"] = run_batched_sharded(sf, dev, rank, world)
+    except Exception as e:  # reported, not fatal; every rank takes the same steps
+        out["batched_sharded"] = {"error": f"{type(e).__name__}: {e}"}
     return out
+
+
+def run_batched_sharded(sf, dev, rank, world, nprob=48, nrhs=4, seed=2024, reps=10):
+    """The batched draw of run_batched (48 problems, 4 right-hand sides, FP64) dealt
+    to the ranks by batch.shard (largest estimated cost first, to the lightest
+    rank): every rank applies its own problems in one graph launch, with no
+    exchange. Time: max over ranks of the device time of `reps` launches."""
+    import torch
+    import torch.distributed as dist
+    from ncihackaton2023_b200.batch import Batch, apply_cost, column_major, shard
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.integers(8, 41)), int(rng.integers(2, 7))) for _ in range(nprob)]
+    mine = shard([apply_cost(n ** 3, p, nrhs) for n, p in specs], world)[rank]
+    ops, X, Y = [], [], []
+    for i in mine:
+        n, p = specs[i]
+        model = sf.CartesianDiscreteModel((0, 1, 0, 1, 0, 1), (n, n, n))
+        V = sf.FESpace(model, p)
+        m = sf.SumFactorizationMap(3, (p,) * 3, (2 * p,) * 3)
+        op = sf.LazyMatrix(m, V, V, sf.Measure(model, 2 * p))
+        ops.append(op)
+        x = column_major(op.n, nrhs, torch.float64, dev)
+        g = torch.Generator(device=dev).manual_seed(seed + i)
+        x.copy_(torch.rand(x.shape, dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+        X.append(x)
+        Y.append(column_major(op.n, nrhs, torch.float64, dev))
+    b = Batch(ops, nrhs) if ops else None
+    if b is not None:
+        b.autotune(X, Y)
+        for _ in range(3):
+            b.apply(X, Y)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        if b is not None:
+            b.apply(X, Y)
+    e1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1) / reps], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dofs = sum((n * p + 1) ** 3 for n, p in specs) * nrhs
+    mine_dofs = torch.tensor([float(sum((specs[i][0] * specs[i][1] + 1) ** 3 for i in mine) * nrhs)],
+                             device=dev)
+    dist.all_reduce(mine_dofs, op=dist.ReduceOp.MAX)
+    return {"problems": nprob, "nrhs": nrhs, "ms_per_apply_max_over_ranks": round(t.item(), 4),
+            "gdof_s": round(dofs / (t.item() * 1e-3) / 1e9, 2),
+            "largest_rank_share": round(mine_dofs.item() / dofs, 4),
+            "sharding": "batch.shard: largest cost first, to the lightest rank; no exchange"}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -347,8 +399,6 @@ def run_ours(args, rank, world, local_rank):
         fn = {"batched": run_batched, "adjoint": run_adjoint, "quad2d": run_quad2d,
               "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,
                                                             cg_iters=args.deformed_cg),
-              "cg_fused": lambda sf_, dev_: run_cg_fused(sf_, dev_, args.cg_candidate,
-                                                         args.cg_maxiter),
               "table_gather": run_table_gather}
         return {args.section: fn[args.section](sf, dev)}
     m, model, V, A = build_problem(sf)
@@ -484,16 +534,8 @@ DO_PARITY = True  # full-size parity checks of the secondary sections (--no-pari
 def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER, mg_modes=True):
     import torch
     res, sols = {}, {}
-    A.set_option("cg_fused", 1)
-    fused = A.info("cg_fused") == 1.0
-    A.set_option("cg_fused", 0)
-    # "jacobi_fused": the same FP64 Jacobi CG with the fused iteration (sf_cg option
-    # cg_fused = 1), for comparison with the default unfused one
-    for mode in ("jacobi", "mixed", "plain") + (("jacobi_fused",) if fused else ()):
-        A.set_option("cg_fused", 1 if mode == "jacobi_fused" else 0)
-        if mode == "jacobi_fused":
-            A.autotune(torch.float64)  # with cg_fused set, also the fused kernel's shapes
-        cg_mode = "jacobi" if mode == "jacobi_fused" else mode
+    for mode in ("jacobi", "mixed", "plain"):
+        cg_mode = mode
         if warm:  # workspaces, diagonal
             sf.cg(A, b, reltol=1e-10, mode=cg_mode, maxiter=maxiter, raise_on_fail=False)
         torch.cuda.synchronize()
@@ -505,8 +547,7 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER, mg_mode
             e1.record()
             torch.cuda.synchronize()
         sols[mode] = x
-        key = {"jacobi": "f64", "mixed": "mixed", "plain": "f64_plain",
-               "jacobi_fused": "f64_fused"}[mode]
+        key = {"jacobi": "f64", "mixed": "mixed", "plain": "f64_plain"}[mode]
         ms = e0.elapsed_time(e1)
         res[key] = {"ms": round(ms, 3), "iters": info["iters"],
                     "ms_per_iter": round(ms / max(1, info["iters"]), 4),
@@ -548,12 +589,6 @@ def _timed_solves(sf, A, b, u_exact=None, warm=True, maxiter=CG_MAXITER, mg_mode
         res["speedup_mg_mixed_vs_f64"] = round(res["f64"]["ms"] / res["mg_mixed"]["ms"], 3)
         res["speedup_mg_mixed_vs_f64_plain"] = round(res["f64_plain"]["ms"] / res["mg_mixed"]["ms"], 3)
         res["speedup_mg_mixed_vs_mg_f64"] = round(res["mg_f64"]["ms"] / res["mg_mixed"]["ms"], 3)
-    if "jacobi_fused" in sols:
-        res["f64_fused"]["iteration"] = A.cg_kernel_name()
-        res["f64_fused"]["err_vs_f64_max_rel"] = (
-            (sols["jacobi_fused"] - sols["jacobi"]).abs().max() / sols["jacobi"].abs().max()).item()
-        res["speedup_fused_vs_unfused"] = round(res["f64"]["ms"] / res["f64_fused"]["ms"], 3)
-    A.set_option("cg_fused", 0)
     res["f64"]["iteration"] = A.cg_kernel_name()
     res["mixed"]["err_vs_f64_max_rel"] = ((sols["mixed"] - sols["jacobi"]).abs().max() /
                                           sols["jacobi"].abs().max()).item()
@@ -819,43 +854,6 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
 # 1024 x 1024 cells, quadrature degree 2(p - 1), GPU sum-factorization kernel
 # gpu_mul_v3! on a V100 (its operator uses the weights only, no geometric factors).
 REF_2D_V100_S = {4: 0.003, 5: 0.0051, 6: 0.00805, 7: 0.014}
-
-
-def run_cg_fused(sf, dev, candidate=None, maxiter=6000):
-    """FP64 Jacobi CG iteration at Q4 64^3, fused (one tile kernel per iteration,
-    sf_cg option cg_fused = 1; every tile shape, or only `candidate`) against the
-    default unfused one: ms per iteration from solves of 60 and 20 iterations on
-    a rough right-hand side (b ~ U[-1,1], seed 1). With maxiter < 20 and a
-    candidate: one fused solve of maxiter iterations only (for a profiler)."""
-    import torch
-    m, model, V, A = build_problem(sf)
-    b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, A.n)).to(dev)
-
-    def solve(k):
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        sf.cg(A, b, reltol=1e-300, maxiter=k, raise_on_fail=False)  # a fixed iteration count
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
-
-    A.set_option("cg_fused", 1)
-    if candidate is not None and maxiter < 20:
-        A.set_option("cg_candidate", candidate)
-        solve(maxiter)
-        return {"iteration": A.cg_kernel_name(), "iters": maxiter}
-    nc = int(A.info("cg_candidates"))
-    out = {}
-    for k in ([candidate] if candidate is not None else list(range(nc))) + [None]:
-        if k is None:
-            A.set_option("cg_fused", 0)
-        else:
-            A.set_option("cg_candidate", k)
-        solve(5)
-        out[A.cg_kernel_name()] = round(min((solve(60) - solve(20)) / 40 for _ in range(2)), 4)
-    log(f"cg ms per iteration: {out}")
-    return {"ms_per_iter": out}
 
 
 def run_table_gather(sf, dev, n=64, p=P, seed=7):

@@ -216,13 +216,8 @@ int sf_diagonal(sf_op* op, int dtype, void* d, void* stream);
  * at profiling/drivers.jl:85-95. Stops when ||r||_2 <= reltol * ||b||_2
  * (FP64 true residual for SF_CG_MIXED). Reports iterations (FP32 iterations
  * for SF_CG_MIXED) and the final relative residual.
- * An FP64 iteration is the apply and two vector kernels. On a whole 3D
- * Cartesian mesh of order 1..8 (the tiled kernel in use), option "cg_fused" = 1
- * selects one fused kernel per iteration instead: the vector updates of
- * iteration k-1 (x, r, and the next direction p) and q = A p in one sweep,
- * with the Jacobi diagonal taken from a per-cell-position table. It moves
- * fewer bytes but is slower on B200 (its loads' latency bounds it). Both
- * are the same CG; iteration counts agree within one.
+ * An FP64 iteration is the apply (which also forms the (p, Ap) sum on the
+ * tiled kernel) and two vector kernels.
  */
 int sf_cg(sf_op* op, int mode, const double* b, double* x, double reltol, int maxiter,
           int* iters, double* relres, void* stream);
@@ -275,9 +270,6 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *   "jacobi_table"        : 1 (default): on a whole 3D Cartesian mesh the FP64 Jacobi CG's
  *                           vector kernels read D^-1 from a table per position in a cell
  *                           (it repeats cell to cell) instead of a vector; 0: from the vector
- *   "cg_fused"            : 1 fused FP64 CG iteration where available, 0 (default) unfused
- *   "cg_candidate"        : force tile-shape candidate k of the fused CG kernel
- *                           (0-based; see sf_get_info "cg_candidates")
  */
 int sf_set_option(sf_op* op, const char* name, double value);
 
@@ -298,16 +290,13 @@ int sf_last_solve_info(const sf_op* op, int* outer, int* inner, double* relres);
  *   "jacobi_table"           : 1 if sf_cg's FP64 Jacobi mode reads D^-1 from the table
  *   "numbered"               : 1 after sf_set_structured_numbering
  *   "numbered_fused"         : 1 if applies read and write through the numbering in the kernel
- *   "cg_fused"               : 1 if sf_cg's FP64 modes use the fused CG kernel
- *   "cg_candidates"          : number of tile shapes of the fused CG kernel
  */
 int sf_get_info(const sf_op* op, const char* key, double* value);
 
 /*
  * Time every tile-shape candidate of the tiled Cartesian kernel for this
  * handle's order, mesh and dtype, and keep the fastest for later sf_apply
- * calls; for SF_F64 with "cg_fused" set, also the fused CG kernel's
- * candidates. Temporary vectors are allocated for the timing. Without the
+ * calls. Temporary vectors are allocated for the timing. Without the
  * tiled kernel (table gather, deformed cells, kappa) it does nothing.
  * Replaces the launch-configuration table that the reference kept by hand
  * (test/benchmark_v3.jl:36-40).

@@ -476,185 +476,6 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
 
 
 // ---------------------------------------------------------------------------
-// Fused FP64 CG pass on the Cartesian operator. One launch carries iteration k
-// of the CG that profiling/drivers.jl:85-95 runs (Jacobi-preconditioned or plain):
-//   r_k = r_{k-1} - alpha q_{k-1},   x_k = x_{k-1} + alpha p_{k-1},
-//   p_k = D^-1 r_k + beta p_{k-1},   q_k = A p_k,
-// with alpha = alpha_{k-1} and beta = beta_{k-1} from the device scalars (both 0
-// on the first pass, which then forms p_0 = D^-1 r_0 and q_0 only). A tile forms
-// p_k on its whole input box, halo included, from the k-1 vectors, and writes
-// x, r and p on its owned points only. The k-1 vectors (r, q, p) are therefore
-// other buffers than the k ones; the caller alternates two sets. A tile
-// computes a halo value with the same operations as the value's owner, so A is
-// applied to exactly the p that is stored.
-// On a Cartesian mesh D^-1 depends only on the position of a point inside its
-// cell (the assembled 1D diagonals repeat with period p), so it comes from a
-// p^3 table in shared memory, not from a vector (all ones for the plain CG).
-// Per tile, in a fixed order, the pass sums
-//   (p_k, q_k), (r_k, D^-1 r_k), (r_k, r_k), (r_k, D^-1 q_k), (q_k, D^-1 q_k).
-// From them the one-block step after the pass forms alpha_k, the stopping test
-// on (r_k, r_k), and beta_k, with (r_{k+1}, D^-1 r_{k+1}) taken one step ahead by
-//   (r - a q, D^-1 (r - a q)) = (r, D^-1 r) - 2a (r, D^-1 q) + a^2 (q, D^-1 q).
-// The exact (r_k, D^-1 r_k) of every pass restarts that recurrence, so its
-// rounding does not build up over the iterations.
-// Memory traffic per pass: r, q, p read on the box, x read on the owned points,
-// x, r, p, q written: eight vector sweeps, against twelve for the apply and the
-// two vector kernels of the unfused iteration.
-// ---------------------------------------------------------------------------
-template <int P>
-struct CgParams {
-  double Me[EO<P>::UE], Mo[EO<P>::UO];
-  double Ke[EO<P>::UE], Ko[EO<P>::UO];
-  double rz, rx, cy;
-  double Kd[P + 1], Md[P + 1], c[3];  // 1D element diagonals and metric: the D^-1 table
-  int jacobi;
-  const double* ab;    // alpha, beta
-  const double* done;  // the pass does nothing once *done >= 2
-  double* partials;    // kCgSums per tile
-  int nfx, nfy, nfz;
-  int ntx, nty;
-};
-
-// FP64 sums of NV values over the CTA, valid in thread 0 (warps added in a fixed order).
-template <int NT, int NV>
-__device__ __forceinline__ void cta_sums(double (&v)[NV]) {
-  __shared__ double red[NV][NT / 32];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-    double t = v[k];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
-    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double t = 0.0;
-#pragma unroll
-      for (int w = 0; w < NT / 32; ++w) t += red[k][w];
-      v[k] = t;
-    }
-  }
-}
-
-// The vectors are separate __restrict__ parameters: none aliases another, so the
-// compiler may keep many loads in flight.
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, bool PAIR, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-k_cartesian_cg(const __grid_constant__ CgParams<P> Q, const double* __restrict__ r_in,
-               const double* __restrict__ q_in, const double* __restrict__ p_in,
-               double* __restrict__ r_out, double* __restrict__ q_out,
-               double* __restrict__ p_out, double* __restrict__ xv) {
-  using T = double;
-  using G = Tile<P, EX, EY, EZ, T>;
-  if (*Q.done >= 2.0) return;  // the same value in every thread
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* T1 = reinterpret_cast<T*>(smem_raw);
-  T* T2 = T1 + G::TS;
-  __shared__ double dtab[P * P * P];  // [lz][ly][lx], l = grid index mod p
-  for (int i = threadIdx.x; i < P * P * P; i += NT) {
-    const int lx = i % P, ly = (i / P) % P, lz = i / (P * P);
-    auto d1 = [&](const double* D, int l) { return l == 0 ? D[0] + D[P] : D[l]; };
-    const double d = Q.c[0] * d1(Q.Kd, lx) * d1(Q.Md, ly) * d1(Q.Md, lz) +
-                     Q.c[1] * d1(Q.Md, lx) * d1(Q.Kd, ly) * d1(Q.Md, lz) +
-                     Q.c[2] * d1(Q.Md, lx) * d1(Q.Md, ly) * d1(Q.Kd, lz);
-    dtab[i] = Q.jacobi ? 1.0 / d : 1.0;
-  }
-  EOMat<P, T> Mm, Km;
-  Mm.load(Q.Me, Q.Mo);
-  Km.load(Q.Ke, Q.Ko);
-  const T alpha = Q.ab[0], beta = Q.ab[1];
-  const int tile = (int)blockIdx.x;
-  const int tx = tile % Q.ntx, ty = (tile / Q.ntx) % Q.nty, tz = tile / (Q.ntx * Q.nty);
-  const int nfx = Q.nfx, nfy = Q.nfy, nfz = Q.nfz;
-  const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
-  const long long pz = (long long)nfx * nfy;
-  const bool interior = fx0 >= 0 && fy0 >= 0 && fz0 >= 0 && fx0 + G::BX <= nfx &&
-                        fy0 + G::BY <= nfy && fz0 + G::BZ <= nfz;
-  __syncthreads();  // dtab
-
-  // ---- z pass input: p_k on the box, from the k-1 vectors (loads only) ----
-  auto load_col = [&](int l, T (&c)[G::BZ]) {
-    const int x = l % G::BX, y = l / G::BX;
-    const int fx = fx0 + x, fy = fy0 + y;
-    const bool inxy = (unsigned)fx < (unsigned)nfx && (unsigned)fy < (unsigned)nfy;
-    const long long col = (long long)fx + (long long)nfx * fy;
-    const double* dcol = dtab + (y % P) * P + (x % P);
-#pragma unroll
-    for (int z = 0; z < G::BZ; ++z) {  // zero inputs (outside the grid) give zero
-      const int fz = fz0 + z;
-      const bool in = interior || (inxy && (unsigned)fz < (unsigned)nfz);
-      const long long i = col + fz * pz;
-      const T r = in ? __ldg(r_in + i) : T(0);
-      const T q = in ? __ldg(q_in + i) : T(0);
-      const T pp = in ? __ldg(p_in + i) : T(0);
-      c[z] = fma(beta, pp, dcol[(z % P) * P * P] * fma(-alpha, q, r));
-    }
-  };
-  tile_passes<P, EX, EY, EZ, NT, ISO, PAIR, T>(T1, T2, Mm, Km, Q.rz, Q.rx, Q.cy, load_col);
-
-  // ---- owned points: r_k and p_k again (the same operations as in the z pass),
-  // x_k, q_k from T1; every write of the pass; the sums ----
-  const int ox0 = fx0 + 1, oy0 = fy0 + 1, oz0 = fz0 + 1;
-  const bool full = ox0 + G::OX <= nfx && oy0 + G::OY <= nfy && oz0 + G::OZ <= nfz;
-  const long long base = (long long)ox0 + (long long)nfx * (oy0 + (long long)nfy * oz0);
-  constexpr int NOUT = G::OX * G::OY * G::OZ;
-  constexpr int PER = (NOUT + NT - 1) / NT;
-  auto point = [&](int k, long long& o, int& t1, int& d) {  // false outside the grid
-    const int i = threadIdx.x + k * NT;
-    const int xo = i % G::OX, r = i / G::OX, yo = r % G::OY, zo = r / G::OY;
-    o = base + xo + (long long)nfx * (yo + (long long)nfy * zo);
-    t1 = zo * G::PLANE + yo * G::RX + xo;
-    d = ((zo + 1) % P) * P * P + ((yo + 1) % P) * P + (xo + 1) % P;
-    return i < NOUT && (full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz));
-  };
-  double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // pq, rz, rr, rq, qq
-  constexpr int CH = PER < 4 ? PER : 4;  // points whose loads are in flight together
-#pragma unroll
-  for (int k0 = 0; k0 < PER; k0 += CH) {
-    T rv[CH], qv[CH], pv[CH], xo[CH];
-#pragma unroll
-    for (int j = 0; j < CH; ++j) {
-      long long o;
-      int t1, d;
-      const bool ok = k0 + j < PER && point(k0 + j, o, t1, d);
-      rv[j] = ok ? __ldg(r_in + o) : T(0);
-      qv[j] = ok ? __ldg(q_in + o) : T(0);
-      pv[j] = ok ? __ldg(p_in + o) : T(0);
-      xo[j] = ok ? xv[o] : T(0);
-    }
-#pragma unroll
-    for (int j = 0; j < CH; ++j) {
-      long long o;
-      int t1, d;
-      if (k0 + j < PER && point(k0 + j, o, t1, d)) {
-        const double dd = dtab[d];
-        const T rn = fma(-alpha, qv[j], rv[j]);
-        const T zr = dd * rn;
-        const T pn = fma(beta, pv[j], zr);
-        const T q = T1[t1];
-        r_out[o] = rn;
-        p_out[o] = pn;
-        q_out[o] = q;
-        xv[o] = fma(alpha, pv[j], xo[j]);
-        const double dq = dd * q;
-        sum[0] = fma(pn, q, sum[0]);
-        sum[1] = fma(rn, zr, sum[1]);
-        sum[2] = fma(rn, rn, sum[2]);
-        sum[3] = fma(rn, dq, sum[3]);
-        sum[4] = fma(q, dq, sum[4]);
-      }
-    }
-  }
-  cta_sums<NT, 5>(sum);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < 5; ++k) Q.partials[(long long)tile * kCgSums + k] = sum[k];
-  }
-}
-
-// ---------------------------------------------------------------------------
 // 2D (quadrilateral Q_p) tiled apply on an nx x ny Cartesian mesh:
 //   y = cx Kx(x)My + cy Mx(x)Ky  (K along the first factor's axis),
 // the 2D form of the Kronecker identity above (the domain of the reference's
@@ -1078,92 +899,6 @@ void run_tile2(const CartesianPlan& plan, const void* x, void* y, const CartFuse
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-// One fused CG pass with the tile configuration (EX, EY, EZ cells, NT threads, MINB CTAs per SM).
-template <int P, int EX, int EY, int EZ, int NT, bool PAIR, int MINB>
-void run_cg(const CartesianPlan& plan, const CgPass& a, cudaStream_t st) {
-  SF_REQUIRE(!plan.slab && plan.D == 3, SF_ERR_UNSUPPORTED,
-             "the fused CG pass runs on a whole 3D mesh only");
-  CgParams<P> Q{};
-  fill_eo<P, double>(plan.M, 1.0, Q.Me, Q.Mo);
-  fill_eo<P, double>(plan.K, 1.0, Q.Ke, Q.Ko);
-  const double cx = plan.c[0], cy = plan.c[1], cz = plan.c[2];
-  Q.rz = cz / cy;
-  Q.rx = cx / cy;
-  Q.cy = cy;
-  const bool iso = (cx == cy) && (cz == cy);
-  for (int l = 0; l <= P; ++l) {
-    Q.Kd[l] = plan.K[l * (P + 1) + l];
-    Q.Md[l] = plan.M[l * (P + 1) + l];
-  }
-  for (int k = 0; k < 3; ++k) Q.c[k] = plan.c[k];
-  Q.jacobi = a.jacobi ? 1 : 0;
-  Q.ab = a.ab;
-  Q.done = a.done;
-  Q.partials = a.partials;
-  Q.nfx = plan.nx * P - 1;
-  Q.nfy = plan.ny * P - 1;
-  Q.nfz = plan.nz * P - 1;
-  Q.ntx = (plan.nx + EX - 1) / EX;
-  Q.nty = (plan.ny + EY - 1) / EY;
-  const long long tiles = (long long)Q.ntx * Q.nty * ((plan.nz + EZ - 1) / EZ);
-  SF_REQUIRE(tiles < (1LL << 31), SF_ERR_ARG, "too many tiles");
-  if (tiles == 0) return;
-  using G = Tile<P, EX, EY, EZ, double>;
-  const size_t smem = (size_t)G::WORDS * sizeof(double);
-  auto kern = iso ? k_cartesian_cg<P, EX, EY, EZ, NT, true, PAIR, MINB>
-                  : k_cartesian_cg<P, EX, EY, EZ, NT, false, PAIR, MINB>;
-  SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<(unsigned)tiles, NT, smem, st>>>(Q, a.r_in, a.q_in, a.p_in, a.r_out, a.q_out, a.p_out,
-                                         a.x);
-  SF_CUDA_CHECK(cudaGetLastError());
-}
-
-struct CgCandidate {
-  void (*run)(const CartesianPlan&, const CgPass&, cudaStream_t);
-  int ex, ey, ez;
-  const char* name;
-};
-#define SF_CGT(P_, EX_, EY_, EZ_, NT_, PAIR_, MINB_)                                        \
-  {&run_cg<P_, EX_, EY_, EZ_, NT_, PAIR_, MINB_>, EX_, EY_, EZ_,                            \
-   "cg pass " #EX_ "x" #EY_ "x" #EZ_ " cells, " #NT_ " thr, " #MINB_ "/SM" ", pair " #PAIR_}
-template <int P>
-struct CgCands;
-#define SF_CGC(P_, ...) \
-  template <> struct CgCands<P_> { static constexpr CgCandidate c[] = {__VA_ARGS__}; };
-SF_CGC(1, SF_CGT(1, 8, 8, 4, 256, true, 2))
-SF_CGC(2, SF_CGT(2, 4, 4, 4, 256, true, 2))
-SF_CGC(3, SF_CGT(3, 4, 4, 2, 256, true, 2))
-SF_CGC(4, SF_CGT(4, 4, 4, 2, 256, false, 3), SF_CGT(4, 4, 4, 2, 256, true, 2))
-SF_CGC(5, SF_CGT(5, 2, 2, 2, 256, false, 2))
-SF_CGC(6, SF_CGT(6, 2, 2, 2, 256, false, 1))
-SF_CGC(7, SF_CGT(7, 2, 2, 1, 256, false, 1))
-SF_CGC(8, SF_CGT(8, 2, 2, 1, 256, false, 1))
-#undef SF_CGC
-#undef SF_CGT
-
-template <int P>
-int cg_cand_count() { return (int)(sizeof(CgCands<P>::c) / sizeof(CgCandidate)); }
-
-int cg_candidates_for(int SB) {
-  switch (SB - 1) {
-#define SF_CASE(P_) \
-  case P_: return cg_cand_count<P_>();
-    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
-#undef SF_CASE
-    default: return 0;
-  }
-}
-
-const CgCandidate& cg_candidate(int SB, int k) {
-  switch (SB - 1) {
-#define SF_CASE(P_) \
-  case P_: return CgCands<P_>::c[k >= 0 && k < cg_cand_count<P_>() ? k : 0];
-    SF_CASE(1) SF_CASE(2) SF_CASE(3) SF_CASE(4) SF_CASE(5) SF_CASE(6) SF_CASE(7) SF_CASE(8)
-#undef SF_CASE
-    default: throw Error(SF_ERR_UNSUPPORTED, "no fused CG pass for this order");
-  }
-}
-
 using RunFn = void (*)(const CartesianPlan&, const void*, void*, const CartFuse&, cudaStream_t);
 using BatchFn = void (*)(const CartesianPlan&, const void*, int, long long, unsigned long long*,
                          bool, cudaStream_t);
@@ -1468,31 +1203,6 @@ long long cartesian_tiles(const CartesianPlan& plan, int dtype) {
   const Candidate& c = pick(plan, dtype, plan.choice[dtype_slot(dtype)]);
   return (long long)((plan.nx + c.ex - 1) / c.ex) * ((plan.ny + c.ey - 1) / c.ey) *
          ((plan.nz + c.ez - 1) / c.ez);
-}
-
-bool cartesian_cg_supported(const CartesianPlan& plan) {
-  return plan.ready && plan.D == 3 && !plan.slab && cg_candidates_for(plan.SB) > 0;
-}
-
-int cartesian_cg_candidates(const CartesianPlan& plan) {
-  return cartesian_cg_supported(plan) ? cg_candidates_for(plan.SB) : 0;
-}
-
-const char* cartesian_cg_candidate_name(const CartesianPlan& plan, int k) {
-  SF_REQUIRE(cartesian_cg_supported(plan), SF_ERR_UNSUPPORTED, "no fused CG pass for this operator");
-  return cg_candidate(plan.SB, k < 0 ? plan.cg_choice : k).name;
-}
-
-long long cartesian_cg_tiles(const CartesianPlan& plan, int k) {
-  SF_REQUIRE(cartesian_cg_supported(plan), SF_ERR_UNSUPPORTED, "no fused CG pass for this operator");
-  const CgCandidate& c = cg_candidate(plan.SB, k < 0 ? plan.cg_choice : k);
-  return (long long)((plan.nx + c.ex - 1) / c.ex) * ((plan.ny + c.ey - 1) / c.ey) *
-         ((plan.nz + c.ez - 1) / c.ez);
-}
-
-void cartesian_cg_pass(const CartesianPlan& plan, int k, const CgPass& a, cudaStream_t stream) {
-  SF_REQUIRE(cartesian_cg_supported(plan), SF_ERR_UNSUPPORTED, "no fused CG pass for this operator");
-  cg_candidate(plan.SB, k < 0 ? plan.cg_choice : k).run(plan, a, stream);
 }
 
 void cartesian_release(CartesianPlan& plan) { plan.ready = false; }

@@ -177,13 +177,18 @@ __device__ __forceinline__ void contract(const T* sMat, const T* sEO, const GenP
 #pragma unroll
     for (int r = 0; r < E::HR; ++r) {
       const V2* t = tab + r * (E::W / 2);
-      T e = E::MC ? (T)t[E::HC].x * u[E::HC] : T(0);
+      // FP32: the table entries come straight from the kernel parameters (an FP32
+      // FMA takes a constant-bank operand), not from shared memory
+      const T* pt = P.eo + EOTables<SB, SQ>::OFF[OP] + r * E::W;
+      constexpr bool kParam = sizeof(T) == 4;
+      T e = E::MC ? (kParam ? pt[2 * E::HC] : (T)t[E::HC].x) * u[E::HC] : T(0);
       T o = T(0);
 #pragma unroll
       for (int i = 0; i < E::HC; ++i) {
-        const V2 eo = t[i];
-        e = fma((T)eo.x, ue[i], e);
-        o = fma((T)eo.y, uo[i], o);
+        const T ex = kParam ? pt[2 * i] : (T)t[i].x;
+        const T ox = kParam ? pt[2 * i + 1] : (T)t[i].y;
+        e = fma(ex, ue[i], e);
+        o = fma(ox, uo[i], o);
       }
       out(r, e + o);
       if (R - 1 - r != r) out(R - 1 - r, anti ? o - e : e - o);

@@ -289,42 +289,6 @@ __global__ void k_cg_direction(double* __restrict__ s, T* __restrict__ x, T* __r
   }
 }
 
-// One block after a fused CG pass: sums [pq, rz, rr, rq, qq] over the tiles,
-// the stopping test on rr, and the next alpha and beta.
-__global__ void k_cg_fused_finish(double* __restrict__ s, const double* __restrict__ partials,
-                                  long long ntiles, int first, double* __restrict__ report) {
-  if (s[CG_DONE] >= 2.0) {
-    if (threadIdx.x == 0) {
-      s[CG_REPORTS] += 1.0;
-      publish(s, report);
-    }
-    return;
-  }
-  double v[5];
-  sum_partials<5>(partials, ntiles, v);
-  if (threadIdx.x != 0) return;
-  const double pq = v[0], rz = v[1], rr = v[2], rq = v[3], qq = v[4];
-  if (!first) s[CG_ITERS] += 1.0;
-  s[CG_PQ] = pq;
-  s[CG_RZ] = rz;
-  s[CG_RR] = rr;
-  if (!isfinite(rr) || !isfinite(rz)) {
-    s[CG_DONE] = 3.0;
-  } else if (rr <= s[CG_TOL2]) {
-    s[CG_DONE] = 2.0;
-  } else {
-    const double alpha = rz / pq;
-    // (r - alpha q, D^-1 (r - alpha q)) for the next pass's r
-    const double rz_next = rz - 2.0 * alpha * rq + alpha * alpha * qq;
-    const double beta = rz_next / rz;
-    if (!isfinite(alpha) || !isfinite(beta)) s[CG_DONE] = 3.0;
-    s[CG_ALPHA] = alpha;
-    s[CG_BETA] = beta;
-  }
-  s[CG_REPORTS] += 1.0;
-  publish(s, report);
-}
-
 // Free-grid position (x, y, z) of a flat index. A grid-stride loop advances it by the
 // position of the stride with one carry per axis, so no division per element.
 struct GridPos {
@@ -683,11 +647,6 @@ void permute_gather(int dtype, const void* x, const int32_t* idx, void* y, long 
   SF_CUDA_CHECK(cudaGetLastError());
 }
 
-void cg_fused_finish(double* s, const double* partials, long long ntiles, bool first,
-                     double* report, cudaStream_t st) {
-  k_cg_fused_finish<<<1, kThreads, 0, st>>>(s, partials, ntiles, first ? 1 : 0, report);
-  SF_CUDA_CHECK(cudaGetLastError());
-}
 
 #define SF_INST(T)                                                                            \
   template void vec_dot<T>(const T*, const T*, long long, double*, double*, double*,            \

@@ -40,6 +40,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "sf_internal.cuh"
@@ -60,23 +61,26 @@ enum MgSlot {
 static_assert(S_COUNTER == 9, "the reduction counter slot of op_apply_dot");
 
 // ---------------------------------------------------------------------------
-// 1D transfer pass along one axis of a structured free-point grid.
-// Prolongation (transpose = 0): the coarse grid has ncc cells of pc points,
-// the fine grid ncc cells of F points along the axis (F = r pf: r fine cells of
-// order pf per coarse cell). Fine point g (grid index 1 .. ncc F - 1) lies in
-// coarse cell c = min(g / F, ncc - 1) at local node l = g - c F, and
+// 1D transfer pass along one axis of a structured free-point grid: out = M in
+// along the axis, with M a sparse (n_out x n_in) matrix in CSR form (start, col,
+// w), the same for every line of the grid.
+// Prolongation from level l+1 to level l: the coarse grid has ncc cells of pc
+// points along the axis, the fine grid ncc cells of F points (F = r pf: r fine
+// cells of order pf per coarse cell). Fine point g (grid index 1 .. ncc F - 1)
+// lies in coarse cell c = min(g / F, ncc - 1) at local node l = g - c F, and
 //     out[g] = sum_m W[l][m] in[c pc + m]      (coarse points 1 .. ncc pc - 1).
-// Restriction (transpose = 1) is the transpose of the same matrix: coarse point
-// j sums W[l_g][j - c_g pc] in[g] over the fine points g of the cells around it,
-// each fine point with the cell the prolongation assigns it to.
+// The restriction is the transpose of that matrix (each fine point with the cell
+// the prolongation assigns it to, so R = P^T exactly). The host builds both
+// matrices per axis once (build_axis).
 // ---------------------------------------------------------------------------
 struct PassParams {
   int n0, n1, n2;        // output grid (x fastest); n1, n2 <= 65535 (grid dimensions)
   int axis;              // 0 x, 1 y, 2 z
   int n_in;              // input points along the axis
-  int ncc, F, pc;
-  int transpose, accumulate, subtract;  // out += ; in - in2
-  double W[kMaxW];       // (F + 1) x (pc + 1), row-major
+  int accumulate, subtract;  // out += ; in - in2
+  const int* start;      // CSR of the 1D matrix: n_out + 1 offsets
+  const int* col;        // input index along the axis (0-based)
+  const double* w;       // weight
 };
 
 template <typename T>
@@ -86,7 +90,6 @@ __global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (i0 >= Q.n0) return;
   const int i1 = blockIdx.y, i2 = blockIdx.z;
-  const int W1 = Q.pc + 1;
   int idx;
   long long base, stride;  // the axis index of the output, input base and stride
   if (Q.axis == 0) {
@@ -99,36 +102,15 @@ __global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict
     base = i0 + Q.n0 * (long long)Q.n_in * i2;
   } else {
     idx = i2;
-    stride = Q.n0 * Q.n1;
+    stride = (long long)Q.n0 * Q.n1;
     base = i0 + Q.n0 * (long long)i1;
   }
-  auto at = [&](int k) {  // input at axis index k (0-based free index)
-    const long long o = base + k * stride;
-    return Q.subtract ? (double)in[o] - (double)in2[o] : (double)in[o];
-  };
+  const int e0 = __ldg(Q.start + idx), e1 = __ldg(Q.start + idx + 1);
   double acc = 0.0;
-  if (!Q.transpose) {
-    const int g = idx + 1;
-    const int c = min(g / Q.F, Q.ncc - 1);
-    const int l = g - c * Q.F;
-    const int top = Q.ncc * Q.pc;
-    for (int m = 0; m <= Q.pc; ++m) {
-      const int j = c * Q.pc + m;
-      const double w = Q.W[l * W1 + m];
-      if (j > 0 && j < top && w != 0.0) acc += w * at(j - 1);
-    }
-  } else {
-    const int gj = idx + 1;
-    const int clo = max(0, (gj + Q.pc - 1) / Q.pc - 1), chi = min(Q.ncc - 1, gj / Q.pc);
-    const int glo = max(1, clo * Q.F), ghi = min(Q.ncc * Q.F - 1, (chi + 1) * Q.F);
-    for (int g = glo; g <= ghi; ++g) {
-      const int c = min(g / Q.F, Q.ncc - 1);
-      const int l = g - c * Q.F;
-      const int m = gj - c * Q.pc;
-      if (m < 0 || m > Q.pc) continue;
-      const double w = Q.W[l * W1 + m];
-      if (w != 0.0) acc += w * at(g - 1);
-    }
+  for (int e = e0; e < e1; ++e) {
+    const long long o = base + (long long)__ldg(Q.col + e) * stride;
+    const double v = Q.subtract ? (double)in[o] - (double)in2[o] : (double)in[o];
+    acc = fma(__ldg(Q.w + e), v, acc);
   }
   const long long o = i0 + Q.n0 * (i1 + Q.n1 * (long long)i2);
   if (Q.accumulate) out[o] = (T)((double)out[o] + acc);
@@ -383,6 +365,10 @@ struct sf_mg {
   struct Transfer {
     int r = 1, F = 0, pc = 0;
     std::vector<double> W;  // (F + 1) x (pc + 1)
+    // device CSR of the 1D prolongation (mode 0) and restriction (mode 1) per axis
+    const int* start[2][3] = {};
+    const int* col[2][3] = {};
+    const double* w[2][3] = {};
   };
   sf_op* A = nullptr;  // the caller's operator (the outer FP64 CG)
   long long n = 0;
@@ -464,28 +450,70 @@ size_t esize(int dtype) { return dtype == SF_F64 ? 8 : 4; }
 // One 1D pass. in/out grids: out dims (n0, n1, n2); the input has n_in points
 // along the axis.
 template <typename T>
-void pass(const sf_mg::Transfer& t, int ncc, int axis, bool transpose, long long n0,
-          long long n1, long long n2, int n_in, const T* in, const T* in2, T* out, bool acc,
-          cudaStream_t st) {
+void pass(const sf_mg::Transfer& t, int axis, bool transpose, long long n0, long long n1,
+          long long n2, int n_in, const T* in, const T* in2, T* out, bool acc, cudaStream_t st) {
   sf::PassParams Q{};
   Q.n0 = (int)n0;
   Q.n1 = (int)n1;
   Q.n2 = (int)n2;
   Q.axis = axis;
   Q.n_in = n_in;
-  Q.ncc = ncc;
-  Q.F = t.F;
-  Q.pc = t.pc;
-  Q.transpose = transpose ? 1 : 0;
   Q.accumulate = acc ? 1 : 0;
   Q.subtract = in2 ? 1 : 0;
-  std::copy(t.W.begin(), t.W.end(), Q.W);
+  const int mode = transpose ? 1 : 0;
+  Q.start = t.start[mode][axis];
+  Q.col = t.col[mode][axis];
+  Q.w = t.w[mode][axis];
   if (n0 <= 0 || n1 <= 0 || n2 <= 0) return;
   SF_REQUIRE(n1 <= 65535 && n2 <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
   const int bx = (int)std::min<long long>(256, (n0 + 31) / 32 * 32);
   const dim3 grid((unsigned)((n0 + bx - 1) / bx), (unsigned)n1, (unsigned)n2);
   sf::k_pass<T><<<grid, bx, 0, st>>>(Q, in, in2, out);
   SF_CUDA_CHECK(cudaGetLastError());
+}
+
+// The 1D prolongation and restriction matrices of transfer t along every axis
+// (ncc coarse cells along each), built on the host and copied to the device.
+void build_tables(sf_mg* mg, sf_mg::Transfer& t, const int ncc[3]) {
+  for (int axis = 0; axis < 3; ++axis) {
+    const int n = ncc[axis], nf = n * t.F - 1, nc = n * t.pc - 1;
+    std::vector<std::vector<std::pair<int, double>>> P(std::max(nf, 0)), R(std::max(nc, 0));
+    for (int g = 1; g < n * t.F; ++g) {
+      const int c = std::min(g / t.F, n - 1);
+      const int l = g - c * t.F;
+      for (int m = 0; m <= t.pc; ++m) {
+        const int j = c * t.pc + m;
+        const double w = t.W[l * (t.pc + 1) + m];
+        if (j > 0 && j < n * t.pc && w != 0.0) {
+          P[g - 1].push_back({j - 1, w});
+          R[j - 1].push_back({g - 1, w});
+        }
+      }
+    }
+    for (int mode = 0; mode < 2; ++mode) {
+      const auto& M = mode == 0 ? P : R;
+      std::vector<int> start(1, 0), col;
+      std::vector<double> w;
+      for (const auto& row : M) {
+        for (const auto& e : row) {
+          col.push_back(e.first);
+          w.push_back(e.second);
+        }
+        start.push_back((int)col.size());
+      }
+      int* ds = static_cast<int*>(mg_alloc(mg, start.size() * sizeof(int)));
+      int* dc = static_cast<int*>(mg_alloc(mg, std::max<size_t>(col.size(), 1) * sizeof(int)));
+      double* dw = static_cast<double*>(mg_alloc(mg, std::max<size_t>(w.size(), 1) * sizeof(double)));
+      SF_CUDA_CHECK(cudaMemcpy(ds, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+      if (!col.empty()) {
+        SF_CUDA_CHECK(cudaMemcpy(dc, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
+        SF_CUDA_CHECK(cudaMemcpy(dw, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+      }
+      t.start[mode][axis] = ds;
+      t.col[mode][axis] = dc;
+      t.w[mode][axis] = dw;
+    }
+  }
 }
 
 // out (fine grid, fx x fy x fz free points) (+)= P in (coarse grid cx x cy x cz);
@@ -499,9 +527,9 @@ void prolong(sf_mg* mg, const sf_mg::Transfer& t, const int ncc[3], const T* in,
                           (long long)ncc[2] * t.F - 1};
   T* a = static_cast<T*>(mg->tmp1);
   T* b = static_cast<T*>(mg->tmp2);
-  pass<T>(t, ncc[2], 2, false, c[0], c[1], f[2], (int)c[2], in, nullptr, a, false, st);
-  pass<T>(t, ncc[1], 1, false, c[0], f[1], f[2], (int)c[1], a, nullptr, b, false, st);
-  pass<T>(t, ncc[0], 0, false, f[0], f[1], f[2], (int)c[0], b, nullptr, out, acc, st);
+  pass<T>(t, 2, false, c[0], c[1], f[2], (int)c[2], in, nullptr, a, false, st);
+  pass<T>(t, 1, false, c[0], f[1], f[2], (int)c[1], a, nullptr, b, false, st);
+  pass<T>(t, 0, false, f[0], f[1], f[2], (int)c[0], b, nullptr, out, acc, st);
 }
 
 // out (coarse) = P^T (in - in2) (fine); in2 may be null.
@@ -514,9 +542,9 @@ void restrict_(sf_mg* mg, const sf_mg::Transfer& t, const int ncc[3], const T* i
                           (long long)ncc[2] * t.F - 1};
   T* a = static_cast<T*>(mg->tmp1);
   T* b = static_cast<T*>(mg->tmp2);
-  pass<T>(t, ncc[0], 0, true, c[0], f[1], f[2], (int)f[0], in, in2, a, false, st);
-  pass<T>(t, ncc[1], 1, true, c[0], c[1], f[2], (int)f[1], a, nullptr, b, false, st);
-  pass<T>(t, ncc[2], 2, true, c[0], c[1], c[2], (int)f[2], b, nullptr, out, false, st);
+  pass<T>(t, 0, true, c[0], f[1], f[2], (int)f[0], in, in2, a, false, st);
+  pass<T>(t, 1, true, c[0], c[1], f[2], (int)f[1], a, nullptr, b, false, st);
+  pass<T>(t, 2, true, c[0], c[1], c[2], (int)f[2], b, nullptr, out, false, st);
 }
 
 template <typename T>
@@ -755,6 +783,8 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
       t.F = r * F.p;
       t.pc = C.p;
       SF_REQUIRE((t.F + 1) * (t.pc + 1) <= sf::kMaxW, SF_ERR_ARG, "transfer table too large");
+      SF_REQUIRE(C.nx <= 65535 && C.ny * t.F <= 65535 && C.nz * t.F <= 65535, SF_ERR_UNSUPPORTED,
+                 "multigrid transfer: grid too large");
       t.W.assign(transfer[l], transfer[l] + (t.F + 1) * (t.pc + 1));
       mg->tr.push_back(t);
     }
@@ -765,6 +795,15 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
       mg->basis.pc = L0.p;
       SF_REQUIRE((L0.p + 1) * (L0.p + 1) <= sf::kMaxW, SF_ERR_ARG, "basis table too large");
       mg->basis.W.assign(basis_change, basis_change + (L0.p + 1) * (L0.p + 1));
+    }
+    for (int l = 0; l + 1 < nlevels; ++l) {
+      const auto& C = mg->lv[l + 1];
+      const int ncc[3] = {C.nx, C.ny, C.nz};
+      build_tables(mg, mg->tr[l], ncc);
+    }
+    if (mg->has_basis) {
+      const int ncc[3] = {L0.nx, L0.ny, L0.nz};
+      build_tables(mg, mg->basis, ncc);
     }
     SF_CUDA_CHECK(cudaStreamCreateWithFlags(&mg->cs, cudaStreamNonBlocking));
     SF_CUDA_CHECK(cudaEventCreateWithFlags(&mg->ev_in, cudaEventDisableTiming));

@@ -18,7 +18,6 @@ struct CartesianPlan {
   // left out when it is the mesh's Dirichlet boundary (slab_top)
   bool slab = false, slab_top = false;
   int D = 3;  // 2: an nx x ny quadrilateral mesh (nz unused)
-  int cg_choice = 0;  // tile candidate of the fused CG pass
 };
 
 // Optional work fused into one apply of the CG loop.
@@ -62,33 +61,5 @@ int cartesian_tile_ez(const CartesianPlan& plan, int dtype);
 // Tiles (CTAs) of one apply with the chosen candidate: the entries CartFuse::dot receives.
 long long cartesian_tiles(const CartesianPlan& plan, int dtype);
 void cartesian_release(CartesianPlan& plan);
-
-// Fused FP64 CG pass (kernels_cartesian.cu, k_cartesian_cg): with alpha, beta of
-// iteration k-1 it forms r_k = r_in - alpha q_in, x += alpha p_in (owned points),
-// p_k = D^-1 r_k + beta p_in and q_k = A p_k into the *_out vectors (which must not
-// alias the *_in ones), and per tile the kCgSums sums
-//   (p_k, q_k), (r_k, D^-1 r_k), (r_k, r_k), (r_k, D^-1 q_k), (q_k, D^-1 q_k).
-// D^-1 is the inverse Jacobi diagonal (jacobi) or the identity.
-constexpr int kCgSums = 5;
-struct CgPass {
-  const double* r_in = nullptr;
-  const double* q_in = nullptr;
-  const double* p_in = nullptr;
-  double* r_out = nullptr;
-  double* q_out = nullptr;
-  double* p_out = nullptr;
-  double* x = nullptr;
-  const double* ab = nullptr;    // alpha, beta
-  const double* done = nullptr;  // the pass does nothing once *done >= 2
-  double* partials = nullptr;    // kCgSums per tile, tile-major
-  bool jacobi = true;
-};
-// Whole 3D meshes of order 1 to 8.
-bool cartesian_cg_supported(const CartesianPlan& plan);
-int cartesian_cg_candidates(const CartesianPlan& plan);
-// k < 0: the plan's cg_choice
-const char* cartesian_cg_candidate_name(const CartesianPlan& plan, int k);
-long long cartesian_cg_tiles(const CartesianPlan& plan, int k);
-void cartesian_cg_pass(const CartesianPlan& plan, int k, const CgPass& a, cudaStream_t stream);
 
 }  // namespace sf

@@ -20,8 +20,6 @@ enum CgSlot {
   CG_PART_PQ = 10,  // distributed CG: this rank's (p, q), then (after the caller's sum) all ranks'
   CG_PART_RZ = 11,  // distributed CG: (r, dinv r), likewise
   CG_PART_RR = 12,  // distributed CG: (r, r), likewise
-  CG_ALPHA = 13,    // fused CG: alpha and beta of the last finished pass (0 before the first)
-  CG_BETA = 14,
   CG_NSLOTS = 16
 };
 
@@ -85,14 +83,6 @@ void cg_update_table(double* s, T* r, const T* q, const JacobiTable& J, long lon
 template <typename T>
 void cg_direction_table(double* s, T* x, T* p, const T* r, const JacobiTable& J, long long n,
                         double* report, cudaStream_t st);
-// After a fused CG pass (cartesian_cg_pass) over ntiles tiles: adds the passes' per-tile
-// sums in a fixed order; RR = (r_k, r_k), RZ, PQ; unless the first pass, ITERS += 1;
-// DONE = 2 once RR <= TOL2 (3 if not finite), else ALPHA = RZ / PQ and BETA from the
-// one-step recurrence for (r_{k+1}, D^-1 r_{k+1}); REPORTS += 1 and a report. Once
-// DONE >= 2 it only reports.
-void cg_fused_finish(double* s, const double* partials, long long ntiles, bool first,
-                     double* report, cudaStream_t st);
-
 // y[i] = x[idx[i]] for a vector of dtype SF_F64 / SF_F32 (n entries, idx a permutation
 // of 0..n-1; the inverse permutation undoes it).
 void permute_gather(int dtype, const void* x, const int32_t* idx, void* y, long long n,

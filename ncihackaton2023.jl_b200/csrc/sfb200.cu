@@ -72,10 +72,6 @@ struct sf_op {
   double* h_report = nullptr;  // mapped pinned: CG progress reports written by the device
   double* d_report = nullptr;  // its device address
   double mixed_inner_reltol = 1e-1;
-  // FP64 CG on the tiled Cartesian operator with one fused pass per iteration. Off by
-  // default: on B200 the fused pass is bound by the latency of its loads (r, q and p over
-  // each tile's halo box), and the unfused iteration is faster.
-  bool cg_fused = false;
   int last_outer = 0, last_inner = 0;
   double last_relres = 0.0;
   std::string err;
@@ -478,65 +474,6 @@ void apply_pq(sf_op* op, const T* p, T* q, double* partials, double* s, cudaStre
   }
 }
 
-bool use_fused_cg(const sf_op* op) {
-  return op->cg_fused && !op->slab && op->n_free > 0 && tiled(op, SF_F64) &&
-         sf::cartesian_cg_supported(op->cart);
-}
-
-// Plain or Jacobi FP64 CG with one fused pass per iteration (cartesian_cg_pass)
-// and a one-block step (cg_fused_finish). Pass k forms x_k, r_k, p_k and
-// q_k = A p_k from the k-1 vectors, which sit in the other of two buffer sets.
-// Pass 0 starts from r_0 = b - A x_0 with alpha = beta = 0, so it only forms
-// p_0 and q_0; x_k is final once (r_k, r_k) meets the tolerance after pass k.
-// maxiter iterations take maxiter + 1 passes.
-int cg_f64_fused(sf_op* op, bool jacobi, const double* b, double* x, double reltol, int maxiter,
-                 double* relres, cudaStream_t st) {
-  const long long n = op->n_free;
-  const long long ntiles = sf::cartesian_cg_tiles(op->cart, -1);
-  const size_t vb = align256(n * sizeof(double));
-  const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
-  const size_t pb = align256(std::max<long long>(3LL * sf::kRedBlocks, sf::kCgSums * ntiles) *
-                             sizeof(double));
-  char* ws = static_cast<char*>(workspace(op, 6 * vb + sb + pb));
-  double* v[6];
-  for (int k = 0; k < 6; ++k) v[k] = reinterpret_cast<double*>(ws + k * vb);
-  double* s = reinterpret_cast<double*>(ws + 6 * vb);
-  double* partials = reinterpret_cast<double*>(ws + 6 * vb + sb);
-  // set k: r = v[3k], q = v[3k + 1], p = v[3k + 2]
-  sf::cg_reset(s, st);  // ALPHA = BETA = 0 for pass 0
-  apply_impl(op, SF_F64, x, v[1], st);
-  sf::cg_start<double>(b, v[1], nullptr, v[0], v[2], n, partials, s, st);  // r_0, p = r_0
-  sf::cg_init(s, reltol * reltol, st);
-  const double* h = read_state(op, s, st);
-  const double bb = h[kBB];
-  const double nb = std::sqrt(bb) > 0 ? std::sqrt(bb) : 1.0;
-  double done = h[kDone];
-  reset_reports(op);
-  sf::CgPass a;
-  a.x = x;
-  a.ab = s + sf::CG_ALPHA;
-  a.done = s + sf::CG_DONE;
-  a.partials = partials;
-  a.jacobi = jacobi;
-  for (int pass = 0; pass <= maxiter && done == 0.0;) {
-    const int in = 3 * (pass & 1), out = 3 - in;
-    a.r_in = v[in];
-    a.q_in = v[in + 1];
-    a.p_in = v[in + 2];
-    a.r_out = v[out];
-    a.q_out = v[out + 1];
-    a.p_out = v[out + 2];
-    sf::cartesian_cg_pass(op->cart, -1, a, st);
-    sf::cg_fused_finish(s, partials, ntiles, pass == 0, op->d_report, st);
-    ++pass;
-    if (pass > kCgLag) done = wait_report(op, pass - kCgLag, st).done;
-  }
-  h = read_state(op, s, st);
-  SF_REQUIRE(h[kDone] != 3.0, SF_ERR_NONFINITE, "non-finite residual in CG");
-  *relres = std::sqrt(h[kRR]) / nb;
-  return (int)h[kIters];
-}
-
 // D^-1 of a whole-mesh 3D Cartesian operator as a p^3 table (sf::JacobiTable), or
 // p = 0 where there is none (the CG then reads a D^-1 vector). The table is the
 // Kronecker-form diagonal of cartesian_diag, inverted, per position in a cell.
@@ -572,7 +509,6 @@ sf::JacobiTable jacobi_table(sf_op* op) {
 // Plain or Jacobi FP64 CG. Returns iterations; sets relres.
 int cg_f64(sf_op* op, bool jacobi, const double* b, double* x, double reltol, int maxiter,
            double* relres, cudaStream_t st) {
-  if (use_fused_cg(op)) return cg_f64_fused(op, jacobi, b, x, reltol, maxiter, relres, st);
   const long long n = op->n_free;
   const size_t vb = align256(n * sizeof(double));
   const size_t sb = align256(sf::CG_NSLOTS * sizeof(double));
@@ -1381,15 +1317,6 @@ int sf_set_option(sf_op* op, const char* name, double value) {
       SF_REQUIRE(value == -1 || value == 0 || value == 1, SF_ERR_ARG,
                  "numbered_fused must be -1 (by the numbering's locality), 0 or 1");
       op->numbered_fused = (int)value;
-    } else if (n == "cg_fused") {
-      SF_REQUIRE(value == 0 || value == 1, SF_ERR_ARG, "cg_fused must be 0 or 1");
-      op->cg_fused = value == 1;
-    } else if (n == "cg_candidate") {
-      const int nc = sf::cartesian_cg_candidates(op->cart);
-      SF_REQUIRE(op->cartesian_ok && nc > 0, SF_ERR_STATE, "the fused CG pass is not in use");
-      SF_REQUIRE(value >= 0 && value < nc && value == (int)value, SF_ERR_ARG,
-                 "CG candidate out of range (0.." + std::to_string(nc - 1) + ")");
-      op->cart.cg_choice = (int)value;
     } else if (n == "tile_candidate_f64" || n == "tile_candidate_f32") {
       const int dt = n == "tile_candidate_f64" ? SF_F64 : SF_F32;
       SF_REQUIRE(op->cartesian_ok, SF_ERR_STATE, "the tiled Cartesian kernel is not in use");
@@ -1421,39 +1348,12 @@ int sf_autotune(sf_op* op, int dtype, void* stream) {
         sf::cartesian_apply_candidate(op->cart, dtype, k, x, y, st);
       });
     }
-    // the fused FP64 CG pass (when selected), on zero vectors with alpha = beta = 0
-    const int ncg = dtype == SF_F64 && op->cg_fused ? sf::cartesian_cg_candidates(op->cart) : 0;
-    if (ncg > 1) {
-      long long tiles = 0;
-      for (int k = 0; k < ncg; ++k) tiles = std::max(tiles, sf::cartesian_cg_tiles(op->cart, k));
-      Scratch sc;
-      const size_t vb = n * sizeof(double);
-      double* zero = static_cast<double*>(sc.get(vb));
-      double* xs = static_cast<double*>(sc.get(vb));
-      double* outs = static_cast<double*>(sc.get(3 * vb));
-      double* sv = static_cast<double*>(sc.get(sf::CG_NSLOTS * sizeof(double)));
-      double* part = static_cast<double*>(sc.get(sf::kCgSums * tiles * sizeof(double)));
-      SF_CUDA_CHECK(cudaMemsetAsync(zero, 0, vb, st));
-      SF_CUDA_CHECK(cudaMemsetAsync(xs, 0, vb, st));
-      SF_CUDA_CHECK(cudaMemsetAsync(sv, 0, sf::CG_NSLOTS * sizeof(double), st));
-      sf::CgPass a;
-      a.r_in = a.q_in = a.p_in = zero;
-      a.r_out = outs;
-      a.q_out = outs + n;
-      a.p_out = outs + 2 * n;
-      a.x = xs;
-      a.ab = sv + sf::CG_ALPHA;
-      a.done = sv + sf::CG_DONE;
-      a.partials = part;
-      op->cart.cg_choice = fastest(ncg, st, [&](int k) { sf::cartesian_cg_pass(op->cart, k, a, st); });
-    }
   });
 }
 
 const char* sf_cg_kernel_name(const sf_op* op) {
   if (!op) return "null handle";
-  if (use_fused_cg(op)) return sf::cartesian_cg_candidate_name(op->cart, -1);
-  return "unfused: apply + vector kernels";
+  return "apply with the (p, Ap) sum, update and direction kernels";
 }
 
 const char* sf_kernel_name(const sf_op* op, int dtype) {
@@ -1474,14 +1374,12 @@ int sf_get_info(const sf_op* op, const char* key, double* value) {
   else if (k == "kernels_per_apply") *value = tiled ? (double)sf::cartesian_launches(op->cart) : 1.0;
   else if (k == "geometry_kind") *value = (double)op->geom.kind;
   else if (k == "slab") *value = op->slab ? 1.0 : 0.0;
-  else if (k == "cg_fused") *value = use_fused_cg(op) ? 1.0 : 0.0;
   else if (k == "numbered") *value = op->d_numbering ? 1.0 : 0.0;
   else if (k == "numbered_fused")
     *value = (op->d_numbering && (op->numbered_fused == 1 ||
                                   (op->numbered_fused < 0 && op->numbering_local))) ? 1.0 : 0.0;
   else if (k == "jacobi_table")
     *value = (op->jacobi_table && !op->slab && tiled && op->D == 3) ? 1.0 : 0.0;
-  else if (k == "cg_candidates") *value = (double)sf::cartesian_cg_candidates(op->cart);
   else if (k == "plane_size") *value = (double)op->plane;
   else if (k == "owned_offset") *value = (double)owned_offset(op);
   else if (k == "owned_count") *value = (double)owned_count(op);

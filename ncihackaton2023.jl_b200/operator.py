@@ -169,6 +169,8 @@ class LazyMatrix:
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
+        for mg in self.__dict__.pop("_mg", {}).values():  # they borrow this handle
+            mg.close()
         if getattr(self, "_h", None):
             lib.sf_destroy(self._h)
             self._h = None
@@ -335,10 +337,22 @@ def cg(A: LazyMatrix, b, x=None, reltol: float = 1e-10, maxiter: int | None = No
     """Solve A x = b on the device (replaces IterativeSolvers.cg! at
     profiling/drivers.jl:85-95). b: float64 CUDA tensor. Returns (x, info)
     with info = {"iters", "relres", "outer", "inner"}. mode: "jacobi" (FP64
-    Jacobi CG), "plain" (FP64 CG, no preconditioner) or "mixed" (FP32 apply
-    and inner CG with FP64 outer refinement)."""
+    Jacobi CG), "plain" (FP64 CG, no preconditioner), "mixed" (FP32 apply
+    and inner CG with FP64 outer refinement), or "mg_mixed" / "mg_f64" (FP64
+    flexible CG preconditioned by a multigrid V-cycle in FP32 / FP64, structured
+    meshes; the hierarchy is built on the first such call and kept on A)."""
+    if mode in ("mg_mixed", "mg_f64"):
+        from .multigrid import Multigrid
+        cache = A.__dict__.setdefault("_mg", {})
+        if mode not in cache:
+            cache[mode] = Multigrid(A, mode=mode[3:])
+        x, info = cache[mode].solve(b, x=x, reltol=reltol,
+                                    maxiter=500 if maxiter is None else int(maxiter),
+                                    raise_on_fail=raise_on_fail)
+        info.update({"outer": 1, "inner": info["iters"]})
+        return x, info
     if mode not in CG_MODES:
-        raise ValueError(f"mode must be one of {sorted(CG_MODES)}")
+        raise ValueError(f"mode must be one of {sorted(CG_MODES) + ['mg_f64', 'mg_mixed']}")
     if b.dtype != torch.float64 or not b.is_cuda or b.numel() != A.n:
         raise ValueError("b must be a float64 CUDA tensor of the operator's size")
     if x is None:

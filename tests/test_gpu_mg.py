@@ -92,3 +92,18 @@ def test_mg_initial_guess_and_cap(sf):
     assert info2["iters"] == 3 and not info2["converged"]
     with pytest.raises(_lib.SumFacError):
         mg.solve(b, reltol=1e-14, maxiter=3)
+
+
+def test_cg_mode_mg(sf):
+    """sf.cg(mode="mg_mixed") builds the hierarchy once and keeps it on the operator."""
+    import torch
+    A, om, mesh = _setup(sf, 2, 6)
+    b = torch.from_numpy(O.rhs(om, mesh, O.sin_forcing)).cuda()
+    x, info = sf.cg(A, b, reltol=1e-10, mode="mg_mixed")
+    assert info["converged"] and info["relres"] <= 1e-10
+    mg = A._mg["mg_mixed"]
+    x2, info2 = sf.cg(A, b, reltol=1e-10, mode="mg_mixed")
+    assert A._mg["mg_mixed"] is mg and torch.equal(x, x2)
+    _check_solution(om, mesh, b.cpu().numpy(), x.cpu().numpy(), 1e-7)
+    A.close()
+    assert mg._h is None
