@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--no-cg", action="store_true", help="skip the CG solves")
     ap.add_argument("--cg-only", action="store_true",
                     help="only the CG solves (autotuned tiles; no apply leg): for profiling")
-    ap.add_argument("--cg-maxiter", type=int, default=6000, help="iteration cap of each CG solve")
+    ap.add_argument("--cg-maxiter", type=int, default=6000,
+                    help="iteration cap of each CG solve (and of the multigrid section's solve)")
     ap.add_argument("--section", choices=["batched", "adjoint", "deformed_q8", "quad2d",
-                                          "table_gather"],
+                                          "table_gather", "multigrid"],
                     default=None,
                     help="run only this secondary configuration (no apply leg): for profiling")
     ap.add_argument("--deformed-cells", type=int, default=32,
@@ -399,7 +400,8 @@ def run_ours(args, rank, world, local_rank):
         fn = {"batched": run_batched, "adjoint": run_adjoint, "quad2d": run_quad2d,
               "deformed_q8": lambda sf_, dev_: run_deformed(sf_, dev_, n=args.deformed_cells,
                                                             cg_iters=args.deformed_cg),
-              "table_gather": run_table_gather}
+              "table_gather": run_table_gather,
+              "multigrid": lambda sf_, dev_: run_multigrid(sf_, dev_, args.cg_maxiter)}
         return {args.section: fn[args.section](sf, dev)}
     m, model, V, A = build_problem(sf)
     if args.cg_only:
@@ -854,6 +856,28 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
 # 1024 x 1024 cells, quadrature degree 2(p - 1), GPU sum-factorization kernel
 # gpu_mul_v3! on a V100 (its operator uses the weights only, no geometric factors).
 REF_2D_V100_S = {4: 0.003, 5: 0.0051, 6: 0.00805, 7: 0.014}
+
+
+def run_multigrid(sf, dev, maxiter=500):
+    """The multigrid CG at Q4 64^3 on the rough right-hand side (b ~ U[-1,1],
+    seed 1), FP32 V-cycle: one warm solve, then one timed solve; with a small
+    maxiter a fixed number of iterations (for a profiler's launch list)."""
+    import torch
+    m, model, V, A = build_problem(sf)
+    b = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, A.n)).to(dev)
+    mg = sf.Multigrid(A, mode="mixed")
+    tol = 1e-10 if maxiter >= 50 else 1e-300
+    mg.solve(b, reltol=tol, maxiter=maxiter, raise_on_fail=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    _, info = mg.solve(b, reltol=tol, maxiter=maxiter, raise_on_fail=False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"ms": round(ms, 3), "iters": info["iters"],
+            "ms_per_iter": round(ms / max(1, info["iters"]), 4), "converged": info["converged"],
+            "levels": [f"Q{q} {c[0]}^3" for q, c in zip(mg.orders, mg.cells)]}
 
 
 def run_table_gather(sf, dev, n=64, p=P, seed=7):

@@ -267,6 +267,9 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *                           through it; 0 x is permuted into lexicographic order and y back;
  *                           -1 (default) 1 when most x-neighbours' ids lie within 64 of each
  *                           other (a cell-by-cell numbering), else 0
+ *   "host_groups"         : sf_mul_host with pinned buffers on the tiled kernel splits the
+ *                           z-levels into this many groups of tile rows, whose copies in,
+ *                           applies and copies out overlap on three streams (default 8)
  *   "jacobi_table"        : 1 (default): on a whole 3D Cartesian mesh the FP64 Jacobi CG's
  *                           vector kernels read D^-1 from a table per position in a cell
  *                           (it repeats cell to cell) instead of a vector; 0: from the vector

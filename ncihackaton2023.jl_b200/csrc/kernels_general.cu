@@ -157,6 +157,12 @@ __device__ __forceinline__ void stage_eo(const GenParams<SB, SQ, T>& P, T* sEO) 
   for (int i = threadIdx.x; i < EOTables<SB, SQ>::TOTAL; i += blockDim.x) sEO[i] = P.eo[i];
 }
 
+// Even-odd table entries read from the kernel parameters (FP32: an FMA takes a
+// constant-bank operand; deformed Q8 0.537 -> 0.464 ms) or from the shared copy
+// (FP64: the parameter reads measured slower, 0.723 -> 0.835 ms at Q8).
+template <typename T>
+constexpr bool kEOParams = sizeof(T) == 4;
+
 // out(r, v) for r < R receives (M u)[r], M one of A, B (OP 0, 1; R = SQ, C = SB) or
 // A^T, B^T (OP 2, 3; R = SB, C = SQ). EO: through the even-odd tables in sEO
 // (about half the FMAs and matrix loads); otherwise the full matrices.
@@ -177,10 +183,8 @@ __device__ __forceinline__ void contract(const T* sMat, const T* sEO, const GenP
 #pragma unroll
     for (int r = 0; r < E::HR; ++r) {
       const V2* t = tab + r * (E::W / 2);
-      // FP32: the table entries come straight from the kernel parameters (an FP32
-      // FMA takes a constant-bank operand), not from shared memory
       const T* pt = P.eo + EOTables<SB, SQ>::OFF[OP] + r * E::W;
-      constexpr bool kParam = sizeof(T) == 4;
+      constexpr bool kParam = kEOParams<T>;
       T e = E::MC ? (kParam ? pt[2 * E::HC] : (T)t[E::HC].x) * u[E::HC] : T(0);
       T o = T(0);
 #pragma unroll

@@ -117,6 +117,28 @@ __global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict
   else out[o] = (T)acc;
 }
 
+// The same pass along x: one block per grid row. The row's inputs (in - in2) are
+// staged in shared memory with coalesced loads, and every output of the row
+// gathers from there.
+template <typename T>
+__global__ void k_pass_x(const __grid_constant__ PassParams Q, const T* __restrict__ in,
+                         const T* __restrict__ in2, T* __restrict__ out) {
+  extern __shared__ double srow[];
+  const int i1 = blockIdx.y, i2 = blockIdx.z;
+  const long long ibase = (long long)Q.n_in * (i1 + Q.n1 * (long long)i2);
+  for (int k = threadIdx.x; k < Q.n_in; k += blockDim.x)
+    srow[k] = Q.subtract ? (double)in[ibase + k] - (double)in2[ibase + k] : (double)in[ibase + k];
+  __syncthreads();
+  const long long obase = (long long)Q.n0 * (i1 + Q.n1 * (long long)i2);
+  for (int i0 = threadIdx.x; i0 < Q.n0; i0 += blockDim.x) {
+    const int e0 = __ldg(Q.start + i0), e1 = __ldg(Q.start + i0 + 1);
+    double acc = 0.0;
+    for (int e = e0; e < e1; ++e) acc = fma(__ldg(Q.w + e), srow[__ldg(Q.col + e)], acc);
+    if (Q.accumulate) out[obase + i0] = (T)((double)out[obase + i0] + acc);
+    else out[obase + i0] = (T)acc;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Chebyshev smoothing steps (first kind) of D^-1 A:
 //   mode 0: d = c2 dinv r,              z = d           (start from z = 0)
@@ -467,8 +489,14 @@ void pass(const sf_mg::Transfer& t, int axis, bool transpose, long long n0, long
   if (n0 <= 0 || n1 <= 0 || n2 <= 0) return;
   SF_REQUIRE(n1 <= 65535 && n2 <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
   const int bx = (int)std::min<long long>(256, (n0 + 31) / 32 * 32);
-  const dim3 grid((unsigned)((n0 + bx - 1) / bx), (unsigned)n1, (unsigned)n2);
-  sf::k_pass<T><<<grid, bx, 0, st>>>(Q, in, in2, out);
+  if (axis == 0 && n_in <= 4096) {  // a row per block, staged in shared memory
+    const int b = (int)std::min<long long>(256, (std::max<long long>(n0, n_in) + 31) / 32 * 32);
+    sf::k_pass_x<T><<<dim3(1, (unsigned)n1, (unsigned)n2), b, (size_t)n_in * sizeof(double), st>>>(
+        Q, in, in2, out);
+  } else {
+    const dim3 grid((unsigned)((n0 + bx - 1) / bx), (unsigned)n1, (unsigned)n2);
+    sf::k_pass<T><<<grid, bx, 0, st>>>(Q, in, in2, out);
+  }
   SF_CUDA_CHECK(cudaGetLastError());
 }
 

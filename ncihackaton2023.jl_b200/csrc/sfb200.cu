@@ -72,6 +72,7 @@ struct sf_op {
   double* h_report = nullptr;  // mapped pinned: CG progress reports written by the device
   double* d_report = nullptr;  // its device address
   double mixed_inner_reltol = 1e-1;
+  int host_groups = 8;  // sf_mul_host: groups of tile rows copied in, applied and copied out
   int last_outer = 0, last_inner = 0;
   double last_relres = 0.0;
   std::string err;
@@ -304,7 +305,7 @@ bool mul_host_pipelined(sf_op* op, const double* x, double* y) {
   const int P = op->p, nz = op->cells.nz;
   const int ez = sf::cartesian_tile_ez(op->cart, SF_F64);
   const int ntz = (nz + ez - 1) / ez;
-  const int groups = std::min(8, ntz);
+  const int groups = std::min(op->host_groups, ntz);
   if (groups < 2) return false;
   const long long plane = op->plane, nfz = (long long)nz * P - 1;
   for (cudaStream_t& q : op->pipe)
@@ -1317,6 +1318,10 @@ int sf_set_option(sf_op* op, const char* name, double value) {
       SF_REQUIRE(value == -1 || value == 0 || value == 1, SF_ERR_ARG,
                  "numbered_fused must be -1 (by the numbering's locality), 0 or 1");
       op->numbered_fused = (int)value;
+    } else if (n == "host_groups") {
+      SF_REQUIRE(value >= 1 && value <= 64 && value == (int)value, SF_ERR_ARG,
+                 "host_groups must be an integer in 1..64");
+      op->host_groups = (int)value;
     } else if (n == "tile_candidate_f64" || n == "tile_candidate_f32") {
       const int dt = n == "tile_candidate_f64" ? SF_F64 : SF_F32;
       SF_REQUIRE(op->cartesian_ok, SF_ERR_STATE, "the tiled Cartesian kernel is not in use");
