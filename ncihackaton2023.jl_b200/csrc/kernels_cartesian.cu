@@ -59,6 +59,20 @@ __host__ __device__ constexpr int tri(int i, int j, int n) {
   return i <= j ? i * n - i * (i - 1) / 2 + (j - i) : j * n - j * (j - 1) / 2 + (i - j);
 }
 
+// A Chebyshev smoothing step fused into the store phase of an apply of z (the
+// kernel's input x): with az = (A z) at an owned point,
+//   d = c2 dinv (r - az) (mode 1) or c1 d + c2 dinv (r - az) (mode 2),  z_out = z + d.
+// z_out must not be z (other tiles still read z's halo).
+template <typename T>
+struct ChebEpi {
+  const T* r;
+  const T* dinv;
+  T* d;
+  T* z_out;
+  T c1, c2;
+  int mode;  // 0: a plain apply
+};
+
 template <int P, typename T>
 struct CartParams {
   T Me[EO<P>::UE], Mo[EO<P>::UO];  // even / odd parts of M
@@ -72,6 +86,7 @@ struct CartParams {
   int tile0;          // first tile of the launch (CTA b applies tile tile0 + b)
   double* dot;  // non-null: dot[tile] = sum of x*y over the tile's outputs
   const int32_t* num;  // numbered kernel: the vectors' index of each lexicographic free point
+  ChebEpi<T> cheb;     // CHEB kernel: the fused Chebyshev step
 };
 
 // FP64 sum over the CTA, valid in thread 0 (adds warps in a fixed order).
@@ -369,14 +384,16 @@ __device__ __forceinline__ void tile_passes(T* T1, T* T2, const EOMat<P, T>& Mm,
 // time; without it they are re-read. NUM: x and y are in another numbering of
 // the free points, num[i] being the index of lexicographic point i; x is read
 // as x[num[i]] and y written as y[num[i]] (no (x, y) sum then).
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, bool NUM = false>
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, bool NUM = false,
+          bool CHEB = false>
 __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
                                           const EOMat<P, T>& Km, const T* __restrict__ X,
                                           T* __restrict__ Y, int nfx, int nfy, int nfz, int zlo,
                                           int nfz_out, int tx,
                                           int ty, int tz, T rz, T rx, T cy,
                                           double* dot = nullptr, T* PS = nullptr,
-                                          const int32_t* __restrict__ num = nullptr) {
+                                          const int32_t* __restrict__ num = nullptr,
+                                          const ChebEpi<T>* cheb = nullptr) {
   using G = Tile<P, EX, EY, EZ, T>;
   // free coordinate of the first input point (grid point e0*p has free index e0*p - 1)
   const int fx0 = tx * EX * P - 1, fy0 = ty * EY * P - 1, fz0 = tz * EZ * P - 1;
@@ -436,6 +453,37 @@ __device__ __forceinline__ void cart_tile(T* T1, T* T2, const EOMat<P, T>& Mm,
     t1 = zo * G::PLANE + yo * G::RX + xo;
     return full || (ox0 + xo < nfx && oy0 + yo < nfy && oz0 + zo < nfz_out);
   };
+  if constexpr (CHEB) {  // the Chebyshev step: all loads of a thread first, then the stores
+    constexpr int PER = (NOUT + NT - 1) / NT;
+    constexpr int CH = PER < 4 ? PER : 4;
+    const ChebEpi<T>& E = *cheb;
+#pragma unroll
+    for (int k0 = 0; k0 < PER; k0 += CH) {
+      T rv[CH], dv[CH], zv[CH], av[CH];
+      long long gv[CH];
+      bool ok[CH];
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        const int i = threadIdx.x + (k0 + j) * NT;
+        long long o;
+        int t1;
+        ok[j] = k0 + j < PER && i < NOUT && out_index(i, o, t1);
+        gv[j] = base + (ok[j] ? o : 0);
+        rv[j] = ok[j] ? __ldg(E.r + gv[j]) - T1[t1] : T(0);
+        av[j] = ok[j] ? __ldg(E.dinv + gv[j]) : T(0);
+        dv[j] = ok[j] && E.mode == 2 ? E.d[gv[j]] : T(0);
+        zv[j] = ok[j] ? __ldg(X + gv[j]) : T(0);
+      }
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        if (!ok[j]) continue;
+        const T v = fma(E.c1, dv[j], E.c2 * av[j] * rv[j]);
+        E.d[gv[j]] = v;
+        E.z_out[gv[j]] = zv[j] + v;
+      }
+    }
+    return;
+  }
   if (!dot) {
     for (int i = threadIdx.x; i < NOUT; i += NT) {
       long long o;
@@ -656,7 +704,8 @@ k_cartesian2d(const __grid_constant__ CartParams2<P, T> Q) {
 template <typename T>
 constexpr bool kStashDot = sizeof(T) == 4;
 
-template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB, bool NUM = false>
+template <int P, int EX, int EY, int EZ, int NT, bool ISO, typename T, int MINB, bool NUM = false,
+          bool CHEB = false>
 __global__ void __launch_bounds__(NT, MINB)
 k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   using G = Tile<P, EX, EY, EZ, T>;
@@ -667,12 +716,11 @@ k_cartesian(const __grid_constant__ CartParams<P, T> Q) {
   Mm.load(Q.Me, Q.Mo);
   Km.load(Q.Ke, Q.Ko);
   const int tile = Q.tile0 + (int)blockIdx.x;
-  cart_tile<P, EX, EY, EZ, NT, ISO, T, NUM>(T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz, Q.zlo,
-                                            Q.nfz_out,
-                                            tile % Q.ntx, (tile / Q.ntx) % Q.nty,
-                                            tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy,
-                                            Q.dot ? Q.dot + tile : nullptr,
-                                            Q.dot && kStashDot<T> ? T2 + G::TS : nullptr, Q.num);
+  cart_tile<P, EX, EY, EZ, NT, ISO, T, NUM, CHEB>(
+      T1, T2, Mm, Km, Q.x, Q.y, Q.nfx, Q.nfy, Q.nfz, Q.zlo, Q.nfz_out, tile % Q.ntx,
+      (tile / Q.ntx) % Q.nty, tile / (Q.ntx * Q.nty), Q.rz, Q.rx, Q.cy,
+      Q.dot ? Q.dot + tile : nullptr, Q.dot && kStashDot<T> ? T2 + G::TS : nullptr, Q.num,
+      &Q.cheb);
 }
 
 // diag(A) on the free points written by an apply (full mesh or slab). On a
@@ -862,6 +910,24 @@ void run_tile(const CartesianPlan& plan, const void* x, void* y, const CartFuse&
   const size_t smem =
       ((size_t)G::WORDS + (fuse.dot && kStashDot<T> ? (size_t)G::OX * G::OY * G::OZ : 0)) *
       sizeof(T);
+  if (fuse.cheb.mode) {  // an apply with the Chebyshev step in its store phase (FP32)
+    SF_REQUIRE(!fuse.dot && fuse.tz1 < 0 && !plan.slab, SF_ERR_UNSUPPORTED,
+               "the Chebyshev store phase takes a whole mesh without a fused dot or row range");
+    if constexpr (sizeof(T) == 4 && !NUM) {
+      SF_REQUIRE(fuse.cheb.z_out != x, SF_ERR_ARG, "the Chebyshev step writes z elsewhere");
+      Q.cheb = ChebEpi<T>{static_cast<const T*>(fuse.cheb.r), static_cast<const T*>(fuse.cheb.dinv),
+                          static_cast<T*>(fuse.cheb.d), static_cast<T*>(fuse.cheb.z_out),
+                          (T)fuse.cheb.c1, (T)fuse.cheb.c2, fuse.cheb.mode};
+      auto kc = iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB, false, true>
+                    : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB, false, true>;
+      SF_CUDA_CHECK(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kc<<<(unsigned)tiles, NT, smem, st>>>(Q);
+      SF_CUDA_CHECK(cudaGetLastError());
+      return;
+    } else {
+      throw Error(SF_ERR_UNSUPPORTED, "the Chebyshev store phase is FP32 only");
+    }
+  }
   auto kern = iso ? k_cartesian<P, EX, EY, EZ, NT, true, T, MINB, NUM>
                   : k_cartesian<P, EX, EY, EZ, NT, false, T, MINB, NUM>;
   SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -83,20 +83,22 @@ struct PassParams {
   const double* w;       // weight
 };
 
+// Blocks of 32 x 8 threads: 32 consecutive outputs along x (threadIdx.x) on 8
+// grid rows (threadIdx.y), so that every warp works on one row.
+constexpr int kPassRows = 8;
+
+// Passes along y or z: each thread one output; the CSR row is the same for the
+// whole warp along y (and for the whole block along z).
 template <typename T>
 __global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict__ in,
                        const T* __restrict__ in2, T* __restrict__ out) {
-  // one thread per output point: x from the block's x index, y and z from the grid
-  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i0 >= Q.n0) return;
-  const int i1 = blockIdx.y, i2 = blockIdx.z;
+  const int i0 = blockIdx.x * 32 + threadIdx.x;
+  const int i1 = blockIdx.y * kPassRows + threadIdx.y;
+  const int i2 = blockIdx.z;
+  if (i0 >= Q.n0 || i1 >= Q.n1) return;
   int idx;
   long long base, stride;  // the axis index of the output, input base and stride
-  if (Q.axis == 0) {
-    idx = i0;
-    stride = 1;
-    base = (long long)Q.n_in * (i1 + Q.n1 * (long long)i2);
-  } else if (Q.axis == 1) {
+  if (Q.axis == 1) {
     idx = i1;
     stride = Q.n0;
     base = i0 + Q.n0 * (long long)Q.n_in * i2;
@@ -117,23 +119,24 @@ __global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict
   else out[o] = (T)acc;
 }
 
-// The same pass along x: one block per grid row. The row's inputs (in - in2) are
-// staged in shared memory with coalesced loads, and every output of the row
-// gathers from there.
+// The pass along x: each warp takes one grid row, stages its inputs (in - in2) in
+// shared memory with coalesced loads, and gathers its outputs from there.
 template <typename T>
 __global__ void k_pass_x(const __grid_constant__ PassParams Q, const T* __restrict__ in,
                          const T* __restrict__ in2, T* __restrict__ out) {
   extern __shared__ double srow[];
-  const int i1 = blockIdx.y, i2 = blockIdx.z;
+  const int i1 = blockIdx.y * kPassRows + threadIdx.y, i2 = blockIdx.z;
+  if (i1 >= Q.n1) return;  // the whole warp
+  double* row = srow + threadIdx.y * Q.n_in;
   const long long ibase = (long long)Q.n_in * (i1 + Q.n1 * (long long)i2);
-  for (int k = threadIdx.x; k < Q.n_in; k += blockDim.x)
-    srow[k] = Q.subtract ? (double)in[ibase + k] - (double)in2[ibase + k] : (double)in[ibase + k];
-  __syncthreads();
+  for (int k = threadIdx.x; k < Q.n_in; k += 32)
+    row[k] = Q.subtract ? (double)in[ibase + k] - (double)in2[ibase + k] : (double)in[ibase + k];
+  __syncwarp();
   const long long obase = (long long)Q.n0 * (i1 + Q.n1 * (long long)i2);
-  for (int i0 = threadIdx.x; i0 < Q.n0; i0 += blockDim.x) {
+  for (int i0 = threadIdx.x; i0 < Q.n0; i0 += 32) {
     const int e0 = __ldg(Q.start + i0), e1 = __ldg(Q.start + i0 + 1);
     double acc = 0.0;
-    for (int e = e0; e < e1; ++e) acc = fma(__ldg(Q.w + e), srow[__ldg(Q.col + e)], acc);
+    for (int e = e0; e < e1; ++e) acc = fma(__ldg(Q.w + e), row[__ldg(Q.col + e)], acc);
     if (Q.accumulate) out[obase + i0] = (T)((double)out[obase + i0] + acc);
     else out[obase + i0] = (T)acc;
   }
@@ -379,7 +382,9 @@ struct sf_mg {
     double* dinv64 = nullptr;  // FP64 D^-1 (set-up)
     void* dinv = nullptr;      // D^-1 in the cycle's type
     void* r = nullptr;         // input (the restricted residual below level 0)
-    void* z = nullptr;         // output
+    void* zb[2] = {nullptr, nullptr};  // output (two buffers: a fused Chebyshev step
+    int cur = 0;                        // writes z + d into the other one); zb[cur] is current
+    void* z() const { return zb[cur]; }
     void* d = nullptr;         // Chebyshev direction
     void* t = nullptr;         // A z
   };
@@ -487,15 +492,16 @@ void pass(const sf_mg::Transfer& t, int axis, bool transpose, long long n0, long
   Q.col = t.col[mode][axis];
   Q.w = t.w[mode][axis];
   if (n0 <= 0 || n1 <= 0 || n2 <= 0) return;
-  SF_REQUIRE(n1 <= 65535 && n2 <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
-  const int bx = (int)std::min<long long>(256, (n0 + 31) / 32 * 32);
-  if (axis == 0 && n_in <= 4096) {  // a row per block, staged in shared memory
-    const int b = (int)std::min<long long>(256, (std::max<long long>(n0, n_in) + 31) / 32 * 32);
-    sf::k_pass_x<T><<<dim3(1, (unsigned)n1, (unsigned)n2), b, (size_t)n_in * sizeof(double), st>>>(
-        Q, in, in2, out);
+  SF_REQUIRE(n2 <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
+  const dim3 block(32, sf::kPassRows);
+  const unsigned gy = (unsigned)((n1 + sf::kPassRows - 1) / sf::kPassRows);
+  if (axis == 0 && n_in <= 768) {  // rows staged in shared memory (8 x n_in doubles)
+    sf::k_pass_x<T><<<dim3(1, gy, (unsigned)n2), block,
+                      (size_t)sf::kPassRows * n_in * sizeof(double), st>>>(Q, in, in2, out);
   } else {
-    const dim3 grid((unsigned)((n0 + bx - 1) / bx), (unsigned)n1, (unsigned)n2);
-    sf::k_pass<T><<<grid, bx, 0, st>>>(Q, in, in2, out);
+    SF_REQUIRE(axis != 0, SF_ERR_UNSUPPORTED, "multigrid transfer: grid rows too long");
+    sf::k_pass<T><<<dim3((unsigned)((n0 + 31) / 32), gy, (unsigned)n2), block, 0, st>>>(
+        Q, in, in2, out);
   }
   SF_CUDA_CHECK(cudaGetLastError());
 }
@@ -579,8 +585,25 @@ template <typename T>
 void cheb_step(int mode, const sf_mg::Level& L, T c1, T c2, cudaStream_t st) {
   sf::k_cheb<T><<<sf::grid_of(L.n), sf::kT, 0, st>>>(
       mode, L.n, static_cast<const T*>(L.r), static_cast<const T*>(L.t),
-      static_cast<const T*>(L.dinv), static_cast<T*>(L.z), static_cast<T*>(L.d), c1, c2);
+      static_cast<const T*>(L.dinv), static_cast<T*>(L.z()), static_cast<T*>(L.d), c1, c2);
   SF_CUDA_CHECK(cudaGetLastError());
+}
+
+// One Chebyshev step after z = zb[cur] (mode 1 or 2): on an FP32 tiled level, fused
+// into the apply's store phase, which writes z + d into the other buffer; otherwise
+// an apply into t and the step kernel.
+template <typename T>
+void cheb_apply_step(sf_mg::Level& L, int dt, int mode, double c1, double c2, cudaStream_t st) {
+  if constexpr (sizeof(T) == 4) {
+    if (sf::op_cheb_apply(L.op, static_cast<const float*>(L.z()), static_cast<const float*>(L.r),
+                          static_cast<const float*>(L.dinv), static_cast<float*>(L.d),
+                          static_cast<float*>(L.zb[L.cur ^ 1]), c1, c2, mode, st)) {
+      L.cur ^= 1;
+      return;
+    }
+  }
+  sf::op_apply(L.op, dt, L.z(), L.t, st);
+  cheb_step<T>(mode, L, T(c1), T(c2), st);
 }
 
 // `deg` Chebyshev steps on level L over [lmax / ratio, 1.1 lmax]; zero_start: z = 0 first.
@@ -589,16 +612,11 @@ void smooth(sf_mg::Level& L, int dt, int deg, double ratio, bool zero_start, cud
   const double b = 1.1 * L.lmax, a = b / (1.1 * ratio);
   const double theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
   double rho = 1.0 / sigma;
-  if (zero_start) {
-    cheb_step<T>(0, L, T(0), T(1.0 / theta), st);
-  } else {
-    sf::op_apply(L.op, dt, L.z, L.t, st);
-    cheb_step<T>(1, L, T(0), T(1.0 / theta), st);
-  }
+  if (zero_start) cheb_step<T>(0, L, T(0), T(1.0 / theta), st);
+  else cheb_apply_step<T>(L, dt, 1, 0.0, 1.0 / theta, st);
   for (int k = 1; k < deg; ++k) {
-    sf::op_apply(L.op, dt, L.z, L.t, st);
     const double rho_n = 1.0 / (2.0 * sigma - rho);
-    cheb_step<T>(2, L, T(rho_n * rho), T(2.0 * rho_n / delta), st);
+    cheb_apply_step<T>(L, dt, 2, rho_n * rho, 2.0 * rho_n / delta, st);
     rho = rho_n;
   }
 }
@@ -611,13 +629,13 @@ void vcycle(sf_mg* mg, int l, int dt, cudaStream_t st) {
     return;
   }
   smooth<T>(L, dt, mg->degree, mg->ratio, true, st);
-  sf::op_apply(L.op, dt, L.z, L.t, st);
+  sf::op_apply(L.op, dt, L.z(), L.t, st);
   sf_mg::Level& C = mg->lv[l + 1];
   const int ncc[3] = {C.nx, C.ny, C.nz};
   restrict_<T>(mg, mg->tr[l], ncc, static_cast<const T*>(L.r), static_cast<const T*>(L.t),
                static_cast<T*>(C.r), st);
   vcycle<T>(mg, l + 1, dt, st);
-  prolong<T>(mg, mg->tr[l], ncc, static_cast<const T*>(C.z), static_cast<T*>(L.z), true, st);
+  prolong<T>(mg, mg->tr[l], ncc, static_cast<const T*>(C.z()), static_cast<T*>(L.z()), true, st);
   smooth<T>(L, dt, mg->degree, mg->ratio, false, st);
 }
 
@@ -630,7 +648,7 @@ void precondition(sf_mg* mg, int dt, cudaStream_t st) {
     restrict_<T>(mg, mg->basis, ncc, static_cast<const T*>(mg->rl), nullptr,
                  static_cast<T*>(L0.r), st);
     vcycle<T>(mg, 0, dt, st);
-    prolong<T>(mg, mg->basis, ncc, static_cast<const T*>(L0.z), static_cast<T*>(mg->zl), false,
+    prolong<T>(mg, mg->basis, ncc, static_cast<const T*>(L0.z()), static_cast<T*>(mg->zl), false,
                st);
   } else {
     vcycle<T>(mg, 0, dt, st);
@@ -659,7 +677,8 @@ void ensure_buffers(sf_mg* mg, int dt) {
   for (size_t l = 0; l < mg->lv.size(); ++l) {
     auto& L = mg->lv[l];
     L.dinv = mg_alloc(mg, L.n * es);
-    L.z = mg_alloc(mg, L.n * es);
+    L.zb[0] = mg_alloc(mg, L.n * es);
+    L.zb[1] = mg_alloc(mg, L.n * es);
     L.d = mg_alloc(mg, L.n * es);
     L.t = mg_alloc(mg, L.n * es);
     L.r = (l == 0 && !mg->has_basis) ? nullptr : mg_alloc(mg, L.n * es);
@@ -671,7 +690,7 @@ void ensure_buffers(sf_mg* mg, int dt) {
     SF_CUDA_CHECK(cudaGetLastError());
   }
   mg->rl = mg_alloc(mg, mg->n * es);
-  mg->zl = mg->has_basis ? mg_alloc(mg, mg->n * es) : mg->lv[0].z;
+  mg->zl = mg->has_basis ? mg_alloc(mg, mg->n * es) : nullptr;  // else level 0's current z
   if (!mg->has_basis) mg->lv[0].r = mg->rl;
   mg->dtype = dt;
 }
@@ -715,7 +734,7 @@ template <typename TL>
 void fcg_iteration(sf_mg* mg, int dt, cudaStream_t st) {
   const long long n = mg->n;
   precondition<TL>(mg, dt, st);
-  const TL* z = static_cast<const TL*>(mg->zl);
+  const TL* z = static_cast<const TL*>(mg->has_basis ? mg->zl : mg->lv[0].z());
   const int g = sf::grid_of(n);
   sf::k_fcg_zq<TL><<<g, sf::kT, 0, st>>>(z, mg->q, n, mg->partials, mg->s);
   sf::k_fcg_dir<TL><<<g, sf::kT, 0, st>>>(z, mg->p, mg->r, n, mg->partials, mg->s);
@@ -811,8 +830,8 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
       t.F = r * F.p;
       t.pc = C.p;
       SF_REQUIRE((t.F + 1) * (t.pc + 1) <= sf::kMaxW, SF_ERR_ARG, "transfer table too large");
-      SF_REQUIRE(C.nx <= 65535 && C.ny * t.F <= 65535 && C.nz * t.F <= 65535, SF_ERR_UNSUPPORTED,
-                 "multigrid transfer: grid too large");
+      SF_REQUIRE(F.nx * F.p <= 768 && F.nz * F.p <= 65535, SF_ERR_UNSUPPORTED,
+                 "multigrid transfer: at most 767 free points per grid row");
       t.W.assign(transfer[l], transfer[l] + (t.F + 1) * (t.pc + 1));
       mg->tr.push_back(t);
     }
@@ -822,6 +841,8 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
       mg->basis.F = L0.p;
       mg->basis.pc = L0.p;
       SF_REQUIRE((L0.p + 1) * (L0.p + 1) <= sf::kMaxW, SF_ERR_ARG, "basis table too large");
+      SF_REQUIRE(L0.nx * L0.p <= 768, SF_ERR_UNSUPPORTED,
+                 "multigrid transfer: at most 767 free points per grid row");
       mg->basis.W.assign(basis_change, basis_change + (L0.p + 1) * (L0.p + 1));
     }
     for (int l = 0; l + 1 < nlevels; ++l) {

@@ -20,6 +20,19 @@ struct CartesianPlan {
   int D = 3;  // 2: an nx x ny quadrilateral mesh (nz unused)
 };
 
+// A Chebyshev smoothing step of the multigrid smoother fused into an FP32 apply of z
+// (the apply's x): with az = (A z) at every point,
+//   d = c2 dinv (r - az) (mode 1) or c1 d + c2 dinv (r - az) (mode 2),  z_out = z + d,
+// and nothing is written to the apply's y. z_out is another buffer than z.
+struct CartCheb {
+  const void* r = nullptr;
+  const void* dinv = nullptr;
+  void* d = nullptr;
+  void* z_out = nullptr;
+  double c1 = 0.0, c2 = 0.0;
+  int mode = 0;  // 0: none
+};
+
 // Optional work fused into one apply of the CG loop.
 struct CartFuse {
   double* dot = nullptr;  // per-tile partial sums of x*y (cartesian_tiles entries)
@@ -27,6 +40,7 @@ struct CartFuse {
   // x and y in another numbering of the free points: num[i] is the index of lexicographic
   // point i (a whole mesh; no dot or tile-row range with it)
   const int32_t* num = nullptr;
+  CartCheb cheb;  // mode != 0: the Chebyshev step instead of writing y (FP32, whole mesh)
 };
 
 // Builds the 1D operators; returns false when no tiled kernel exists for SB.

@@ -95,5 +95,10 @@ void op_diag(sf_op* op, double* d, cudaStream_t st);
 void op_apply_dot(sf_op* op, const double* x, double* y, double* partials, double* out, double* s,
                   const double* skip, cudaStream_t st);
 long long op_dot_partials(const sf_op* op);
+// A Chebyshev step fused into an FP32 apply of z on the tiled kernel: d = c2 dinv (r - A z)
+// (mode 1) or c1 d + c2 dinv (r - A z) (mode 2), z_out = z + d. Returns false (and does
+// nothing) when the operator does not run the tiled kernel.
+bool op_cheb_apply(sf_op* op, const float* z, const float* r, const float* dinv, float* d,
+                   float* z_out, double c1, double c2, int mode, cudaStream_t st);
 
 }  // namespace sf

@@ -1875,5 +1875,20 @@ void op_apply_dot(sf_op* op, const double* x, double* y, double* partials, doubl
 
 long long op_dot_partials(const sf_op* op) { return cg_partials(op); }
 
+bool op_cheb_apply(sf_op* op, const float* z, const float* r, const float* dinv, float* d,
+                   float* z_out, double c1, double c2, int mode, cudaStream_t st) {
+  if (!tiled(op, SF_F32) || op->d_numbering || op->slab || op->n_free == 0) return false;
+  sf::CartFuse fuse;
+  fuse.cheb.r = r;
+  fuse.cheb.dinv = dinv;
+  fuse.cheb.d = d;
+  fuse.cheb.z_out = z_out;
+  fuse.cheb.c1 = c1;
+  fuse.cheb.c2 = c2;
+  fuse.cheb.mode = mode;
+  sf::cartesian_apply(op->cart, SF_F32, z, nullptr, st, fuse);
+  return true;
+}
+
 
 }  // namespace sf
