@@ -155,6 +155,19 @@ def build_problem(sf):
     return m, model, V, A
 
 
+# count_manual_flops_poisson_matrix_free(1, 3, (9,)*3, (9,)*3, count_only_fma_ops=false,
+# structured_mesh_opt=false) of src/Utils.jl:33-72: flops per deformed Q8 cell
+Q8_DEFORMED_FLOPS_PER_CELL = 352107
+
+
+def HBM_PEAK_GBS():
+    """The measured copy bandwidth of MEASURED_PEAKS.json, else the fallback figure."""
+    try:
+        return float(json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
 def roofline_entry(achieved_gbs, peaks, traffic):
     peak = peaks.get("hbm_gbs") if peaks else None
     src = "measured" if peak else "fallback"
@@ -786,14 +799,23 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
     nq = (p + 1) ** 3
     gbytes = n ** 3 * nq * 6 * 8
     ys_ = {}
+    # the reference's flop model (src/Utils.jl:33-72) for Q8, 9 points, deformed cells
+    model_gflop = n ** 3 * Q8_DEFORMED_FLOPS_PER_CELL / 1e9 if p == 8 else float("nan")
     for dt, key, vb in ((torch.float64, "f64", 8), (torch.float32, "f32", 4)):
         xx, yy = x.to(dt), y.to(dt)
         for _ in range(3):
             sf.mul(yy, A, xx)
         ms = _events_ms(lambda: sf.mul(yy, A, xx), 10)
         byts = gbytes + (n * p + 1) ** 3 * 2 * vb
+        # reference-model flops (src/Utils.jl:33-72, deformed cells: structured_mesh_opt false)
+        # against the nominal vector-pipe peak at 1965 MHz (148 SMs x 64 FP64 / 128 FP32 FMA per clock)
+        tf = model_gflop / ms  # GFLOP / ms = TFLOP/s
+        peak = 148 * (64 if key == "f64" else 128) * 2 * 1.965e9 / 1e12
         res[key] = {"ms": round(ms, 3), "gdof_s": round((n * p + 1) ** 3 / (ms * 1e-3) / 1e9, 2),
-                    "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1)}
+                    "alg_bytes": byts, "achieved_gbs": round(byts / (ms * 1e-3) / 1e9, 1),
+                    "hbm_frac": round(byts / (ms * 1e-3) / 1e9 / HBM_PEAK_GBS(), 4),
+                    "model_tflops": round(tf, 2), "model_tflops_frac_of_nominal_pipe":
+                        round(tf / peak, 3), "nominal_pipe_tflops": round(peak, 1)}
         ys_[key] = yy.double().cpu().numpy()
     if DO_PARITY:  # the full-size applies against the C restatement (chunked geometry)
         from oracle import cref

@@ -246,3 +246,14 @@ def test_adjoint_gradient_matches_finite_differences():
     Jm = O.adjoint_gradient_sparse(m, mesh, b, u_obs, kappa - eps * d, cq)[0]
     fd = (Jp - Jm) / (2 * eps)
     assert abs(fd - np.sum(g * d)) < 1e-6 * abs(fd)
+
+
+def test_bench_flop_constants_match_the_reference_model():
+    """The flop figures bench.py reports come from the reference's model
+    (src/Utils.jl:33-72): Q4 affine (5.997 GFLOP per 64^3 apply) and Q8 deformed."""
+    import bench
+    f = O.count_manual_flops_poisson_matrix_free
+    assert bench.Q8_DEFORMED_FLOPS_PER_CELL == f(1, 3, (9,) * 3, (9,) * 3, count_only_fma_ops=False,
+                                                 structured_mesh_opt=False)
+    assert abs(64 ** 3 * f(1, 3, (5,) * 3, (5,) * 3, count_only_fma_ops=False,
+                           structured_mesh_opt=True) / 1e9 - 5.996544) < 1e-9
