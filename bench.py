@@ -536,9 +536,45 @@ def run_ours(args, rank, world, local_rank):
         out["cg"] = run_cg(sf, m, model, V, A, dev, args.cg_maxiter)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline_port()
+    out["summary"] = summarize(out)
     if world > 1:
         dist.barrier()
     return out
+
+
+def summarize(out):
+    """The solver and form results of the sections in a few lines (ms, iterations)."""
+    def pick(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    def solve(d):
+        if not isinstance(d, dict):
+            return None
+        return {k: d.get(k) for k in ("ms", "iters", "converged") if k in d}
+    summ = {"apply_gdof_s": out.get("value"), "roofline_frac": pick(out, "roofline", "frac"),
+            "parity_pass": pick(out, "parity", "pass")}
+    cg = out.get("cg")
+    if isinstance(cg, dict):
+        for rhs, d in (("manufactured", cg), ("rough", cg.get("rough_rhs"))):
+            summ[f"cg_{rhs}"] = {k: solve(pick(d, k)) for k in ("f64", "f64_plain", "mixed",
+                                                             "mg_f64", "mg_mixed")}
+    dq = out.get("deformed_q8")
+    if isinstance(dq, dict):
+        summ["deformed_q8"] = {"apply_ms": {k: pick(dq, k, "ms") for k in ("f64", "f32")},
+                               "parity_pass": pick(dq, "parity", "pass"),
+                               "mg_mixed": solve(dq.get("cg_mg_mixed")),
+                               "mg_f64": solve(dq.get("cg_mg_f64")),
+                               "jacobi_f64_1500_converged": pick(dq, "cg_f64", "converged")}
+    bt = out.get("batched")
+    if isinstance(bt, dict):
+        summ["batched_ms"] = {k: pick(bt, k, "ms_graph") for k in ("f64", "f32")}
+        summ["batched_parity_pass"] = all(pick(bt, k, "parity", "pass") is not False
+                                          for k in ("f64", "f32"))
+    return summ
 
 
 CG_MAXITER = 6000

@@ -356,16 +356,6 @@ int grid_of(long long n) {
   return (int)std::max(1LL, std::min<long long>((n + kT - 1) / kT, kMgBlocks));
 }
 
-struct Buf {
-  void* p = nullptr;
-  ~Buf() {
-    if (p) cudaFree(p);
-  }
-  void* get(size_t bytes) {
-    if (!p) SF_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
-    return p;
-  }
-};
 
 }  // namespace
 }  // namespace sf

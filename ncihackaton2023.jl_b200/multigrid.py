@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import _lib, fem
-from ._lib import check, lib
+from ._lib import lib
 from .operator import LazyMatrix, SumFactorizationMap, _f64, _stream
 
 MODES = {"mixed": _lib.SF_MG_MIXED, "f64": _lib.SF_MG_F64}
@@ -97,7 +97,6 @@ class Multigrid:
                 model = model.coarsened()
                 levels.append((model, 1, 2))
         self.levels = []
-        self._keep = []
         for l, (mdl, q, _) in enumerate(levels):
             if l == 0 and fam == "equispaced":
                 self.levels.append(A)
