@@ -20,6 +20,8 @@ Hierarchy, finest first:
     through those vertices).
 The transfer tables are 1D Lagrange interpolation matrices between the levels'
 node sets; the library applies them as tensor products along the three axes.
+With a variable coefficient kappa on the operator, every coarse level gets each
+cell's mean of kappa (averaged again over the children of a coarse cell).
 """
 from __future__ import annotations
 
@@ -74,8 +76,6 @@ class Multigrid:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         if A.gather != "structured" or A.m.D != 3:
             raise NotImplementedError("the multigrid hierarchy needs a 3D structured operator")
-        if A.kappa is not None:
-            raise NotImplementedError("the multigrid hierarchy has no variable coefficient")
         p = A.m.order
         if basis == "auto":
             basis = "gll" if p >= 5 else "equispaced"
@@ -116,6 +116,8 @@ class Multigrid:
         if fam == "gll":  # levels[0]'s GLL basis functions at A's equispaced nodes
             basis_tab = _f64(_lagrange_values(nodes(p), np.linspace(0.0, 1.0, p + 1)))
         self._basis_tab = basis_tab
+        if A.kappa is not None:
+            self._set_coefficients(levels)
         ops = (C.c_void_p * len(self.levels))(*[L._h for L in self.levels])
         tab = (C.c_void_p * max(1, len(tables)))(*[t.ctypes.data for t in tables])
         for L in self.levels:  # tile shapes of the level kernels, picked once here
@@ -131,6 +133,31 @@ class Multigrid:
         self.set_option("degree", degree)
         self.set_option("ratio", ratio)
         self.set_option("coarse_steps", coarse_steps)
+
+    def _set_coefficients(self, levels):
+        """A variable coefficient on the coarse levels: the operator's kappa itself on a
+        level with its quadrature, else each cell's mean of it (averaged over the 8
+        children of a coarse cell on the h-levels), constant over the level's points."""
+        A = self.A
+        kap = A.kappa
+        if not isinstance(kap, torch.Tensor):
+            kap = torch.from_numpy(np.ascontiguousarray(kap))
+        kap = kap.to("cuda", torch.float64)
+        cell = kap.mean(dim=1)  # (ncells,), cells x fastest
+        part = tuple(A.model.partition)
+        for l, ((mdl, q, r), L) in enumerate(zip(levels, self.levels)):
+            if L is A:
+                continue
+            if r == 2:  # the coarse cell's mean of its 8 children
+                nx, ny, nz = part
+                cell = cell.reshape(nz // 2, 2, ny // 2, 2, nx // 2, 2).mean(dim=(1, 3, 5))
+                cell = cell.reshape(-1).contiguous()
+                part = (nx // 2, ny // 2, nz // 2)
+            nq = L.m.SQ[0] ** 3
+            if L.m.quad_degree == A.m.quad_degree and mdl is A.model:
+                L.set_coefficient(kap)  # the same points: the operator's own kappa
+            else:
+                L.set_coefficient(cell[:, None].expand(-1, nq).contiguous())
 
     def close(self):
         if getattr(self, "_h", None):

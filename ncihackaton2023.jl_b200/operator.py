@@ -202,7 +202,11 @@ class LazyMatrix:
     # -- extras -----------------------------------------------------------
     def set_coefficient(self, kappa):
         """kappa at every quadrature point, shape (ncells, SQ^3), or None. A float64
-        CUDA tensor is copied on the device; anything else is read on the host."""
+        CUDA tensor is copied on the device; anything else is read on the host.
+        Multigrid hierarchies kept for cg(mode="mg_...") are dropped (their levels
+        hold the previous coefficient)."""
+        for mg in self.__dict__.pop("_mg", {}).values():
+            mg.close()
         if kappa is None:
             check(lib.sf_set_coefficient(self._h, None), self._h, "sf_set_coefficient")
             self.kappa = None

@@ -107,3 +107,31 @@ def test_cg_mode_mg(sf):
     _check_solution(om, mesh, b.cpu().numpy(), x.cpu().numpy(), 1e-7)
     A.close()
     assert mg._h is None
+
+
+def test_mg_variable_coefficient(sf):
+    """-div(kappa grad u) with a rough kappa per quadrature point (exp of N(0, 0.5^2)):
+    the coarse levels take cell means of kappa; the solve is against the oracle's
+    assembled matrix with the same kappa."""
+    import scipy.sparse.linalg as spla
+    import torch
+    p, n = 3, 4
+    A, om, mesh = _setup(sf, p, n)
+    nq = (p + 1) ** 3
+    kappa = np.exp(np.random.default_rng(4).normal(0.0, 0.5, (n ** 3, nq)))
+    A.set_coefficient(torch.from_numpy(kappa).cuda())
+    b = O.rhs(om, mesh, O.sin_forcing)
+    x, info = sf.cg(A, torch.from_numpy(b).cuda(), reltol=1e-10, mode="mg_mixed")
+    assert info["converged"] and info["iters"] <= 40, info
+    As = O.assembled_sparse(om, mesh, kappa=kappa).tocsc()
+    x_ref = spla.spsolve(As, b)
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(b - As @ xs) / np.linalg.norm(b) < 1e-9
+    assert np.abs(xs - x_ref).max() / np.abs(x_ref).max() < 1e-7
+    # a new coefficient drops the kept hierarchy
+    assert "mg_mixed" in A._mg
+    A.set_coefficient(torch.from_numpy(kappa * 2.0).cuda())
+    assert "_mg" not in A.__dict__
+    x2, info2 = sf.cg(A, torch.from_numpy(b).cuda(), reltol=1e-10, mode="mg_mixed")
+    assert info2["converged"]
+    assert np.abs(x2.cpu().numpy() - x_ref / 2.0).max() / np.abs(x_ref / 2.0).max() < 1e-7
