@@ -805,14 +805,26 @@ def run_adjoint(sf, dev, n=32, p=3, seed=11):
     J, grad, u, info = objective_gradient(A, b, u_obs, kappa, reltol=1e-11)
     torch.cuda.synchronize()
     grad_s = time.perf_counter() - t0
-    # the same gradient with multigrid-preconditioned solves (the hierarchy is built for
-    # this kappa inside the first solve; that set-up is included)
+    # a second coefficient, as the next step of an optimisation loop would set
+    kappa_b = kappa * torch.exp(0.1 * torch.from_numpy(rng.normal(0, 1, (nc, nq))).to(dev))
+    _, grad_b, _, _ = objective_gradient(A, b, u_obs, kappa_b, reltol=1e-11)
+    # the same gradients with multigrid-preconditioned solves: at kappa the hierarchy is
+    # built inside the first solve (that set-up is included); at kappa_b the kept
+    # hierarchy follows the new coefficient (Multigrid.refresh, included)
     t0 = time.perf_counter()
     J_mg, grad_mg, _, info_mg = objective_gradient(A, b, u_obs, kappa, reltol=1e-11,
                                                    mode="mg_mixed", maxiter=500)
     torch.cuda.synchronize()
     grad_mg_s = time.perf_counter() - t0
     grad_mg_diff = ((grad_mg - grad).abs().max() / grad.abs().max()).item()
+    t0 = time.perf_counter()
+    _, grad_mg_b, _, info_mg_b = objective_gradient(A, b, u_obs, kappa_b, reltol=1e-11,
+                                                    mode="mg_mixed", maxiter=500)
+    torch.cuda.synchronize()
+    grad_mg_next_s = time.perf_counter() - t0
+    grad_mg_next_diff = ((grad_mg_b - grad_b).abs().max() / grad_b.abs().max()).item()
+    for mg in A.__dict__.pop("_mg", {}).values():  # the checks below use Jacobi CG
+        mg.close()
     d = torch.from_numpy(rng.normal(0, 1, (nc, nq))).to(dev)
     eps = 1e-6
     fd = (objective(A, b, u_obs, kappa + eps * d, 1e-11) -
@@ -823,6 +835,8 @@ def run_adjoint(sf, dev, n=32, p=3, seed=11):
             "gradient_s": round(grad_s, 4), "cg_iters": info, "J": J,
             "gradient_mg_s": round(grad_mg_s, 4), "mg_iters": info_mg,
             "gradient_mg_vs_jacobi_max_rel": grad_mg_diff,
+            "gradient_mg_next_kappa_s": round(grad_mg_next_s, 4), "mg_next_iters": info_mg_b,
+            "gradient_mg_next_vs_jacobi_max_rel": grad_mg_next_diff,
             "fd_directional": fd, "adjoint_directional": ad,
             "fd_rel_err": abs(fd - ad) / abs(fd)}
 
@@ -843,7 +857,6 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
     res = {"mesh": f"{n}^3 Q{p}, {p + 1}-pt Gauss, perturbed 0.2h", "n_free": A.n,
            "setup_s": round(setup_s, 2), "kernel": A.kernel_name()}
     nq = (p + 1) ** 3
-    gbytes = n ** 3 * nq * 6 * 8
     ys_ = {}
     # the reference's flop model (src/Utils.jl:33-72) for Q8, 9 points, deformed cells
     model_gflop = n ** 3 * Q8_DEFORMED_FLOPS_PER_CELL / 1e9 if p == 8 else float("nan")
@@ -852,7 +865,8 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
         for _ in range(3):
             sf.mul(yy, A, xx)
         ms = _events_ms(lambda: sf.mul(yy, A, xx), 10)
-        byts = gbytes + (n * p + 1) ** 3 * 2 * vb
+        # the per-point metric (6 values, in the kernel's type) and x, y
+        byts = n ** 3 * nq * 6 * vb + (n * p + 1) ** 3 * 2 * vb
         # reference-model flops (src/Utils.jl:33-72, deformed cells: structured_mesh_opt false)
         # against the nominal vector-pipe peak at 1965 MHz (148 SMs x 64 FP64 / 128 FP32 FMA per clock)
         tf = model_gflop / ms  # GFLOP / ms = TFLOP/s

@@ -366,6 +366,13 @@ const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int group);
  * one mode. Options (sf_mg_set_option): "degree" (Chebyshev smoothing steps, 3),
  * "ratio" (smoothing range lmax/ratio..1.1 lmax, 30), "coarse_steps" (10),
  * "coarse_ratio" (100). sf_mg_get_info: "levels", "lmax<l>", "n<l>", "graph".
+ *
+ * sf_mg_refresh: after the operators' coefficients changed (sf_set_coefficient
+ * on A and on the levels), recomputes every level's diagonal and eigenvalue
+ * estimate and captures the iteration again on the next solve; the levels,
+ * tables and buffers are kept. Ordered after the work queued on `stream`;
+ * returns when the set-up has finished. Until it succeeds, sf_mg_cg returns
+ * SF_ERR_STATE.
  */
 #define SF_MG_MIXED 0
 #define SF_MG_F64 1
@@ -378,6 +385,7 @@ int sf_mg_set_option(sf_mg* mg, const char* name, double value);
 int sf_mg_get_info(const sf_mg* mg, const char* key, double* value);
 int sf_mg_cg(sf_mg* mg, int mode, const double* b, double* x, double reltol, int maxiter,
              int* iters, double* relres, void* stream);
+int sf_mg_refresh(sf_mg* mg, void* stream);
 
 /*
  * sf_cg_noalloc: sf_cg without any device or pinned-host allocation. It has no

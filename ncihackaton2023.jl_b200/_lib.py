@@ -91,6 +91,7 @@ SIGNATURES = {
     "sf_mg_set_option": (i32, [vp, C.c_char_p, C.c_double]),
     "sf_mg_get_info": (i32, [vp, C.c_char_p, dp]),
     "sf_mg_cg": (i32, [vp, i32, vp, vp, C.c_double, i32, C.POINTER(i32), dp, vp]),
+    "sf_mg_refresh": (i32, [vp, vp]),
 }
 
 SF_NOALLOC_MAX_FREE = 262144

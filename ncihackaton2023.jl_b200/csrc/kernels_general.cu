@@ -17,6 +17,7 @@
 // __grid_constant__ parameters (staged in shared memory for FP64 at high order,
 // see kStageMats). The scatter-add uses atomics into a y that was zeroed before
 // the launch. Dirichlet dofs (id < 0) read as zero and are skipped.
+#include <algorithm>
 #include <cmath>
 #include <type_traits>
 
@@ -59,6 +60,8 @@ struct GenParams {
   int geom;             // GEOM_SEPARABLE / GEOM_TABLE
   const double* gtab;
   long long gstride;
+  const float* gtab32;  // FP32 copy of gtab (read by the FP32 kernel)
+  long long gstride32;
   const double* kappa;
   const double* wdet;
   long long wdet_stride;
@@ -315,30 +318,37 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
       load(zz, ZS, u);
       contract<1, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { zz[r * ZS] = v; });
     }
-    // metric in FP64 (geometric factors are kept in FP64 for both dtypes)
-    const double* gt = P.geom == GEOM_SEPARABLE ? nullptr : P.gtab + (valid ? cell : 0) * P.gstride;
+    // metric v = G u in the kernel's type: the FP64 kernel reads the FP64 table, the
+    // FP32 kernel its FP32 copy (half the bytes of the largest stream)
+    const long long gc = valid ? cell : 0;
+    const double* gt = P.geom == GEOM_SEPARABLE || sizeof(T) == 4 ? nullptr : P.gtab + gc * P.gstride;
+    const float* gt32 = P.geom == GEOM_SEPARABLE || sizeof(T) == 8 ? nullptr
+                                                                   : P.gtab32 + gc * P.gstride32;
 #pragma unroll 3
     for (int qk = 0; qk < SQ; ++qk) {
       const int q = qi + SQ * (qj + SQ * qk);
-      double g[6];
+      T g[6];
       asm volatile("" ::: "memory");
       if (P.geom == GEOM_SEPARABLE) {
         const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
 #pragma unroll
-        for (int c = 0; c < 6; ++c) g[c] = s * P.G0[c];
+        for (int c = 0; c < 6; ++c) g[c] = (T)(s * P.G0[c]);
+      } else if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) g[c] = __ldg(gt32 + c * SQ * SQ * SQ + q);
       } else {
 #pragma unroll
         for (int c = 0; c < 6; ++c) g[c] = __ldg(gt + c * SQ * SQ * SQ + q);
       }
       if (P.kappa) {
-        const double kq = valid ? P.kappa[cell * (SQ * SQ * SQ) + q] : 0.0;
+        const T kq = valid ? (T)P.kappa[cell * (SQ * SQ * SQ) + q] : T(0);
 #pragma unroll
         for (int c = 0; c < 6; ++c) g[c] *= kq;
       }
-      const double dx = (double)zx[qk * ZS], dy = (double)zy[qk * ZS], dz = (double)zz[qk * ZS];
-      zx[qk * ZS] = (T)(g[0] * dx + g[3] * dy + g[4] * dz);
-      zy[qk * ZS] = (T)(g[3] * dx + g[1] * dy + g[5] * dz);
-      zz[qk * ZS] = (T)(g[4] * dx + g[5] * dy + g[2] * dz);
+      const T dx = zx[qk * ZS], dy = zy[qk * ZS], dz = zz[qk * ZS];
+      zx[qk * ZS] = g[0] * dx + g[3] * dy + g[4] * dz;
+      zy[qk * ZS] = g[3] * dx + g[1] * dy + g[5] * dz;
+      zz[qk * ZS] = g[4] * dx + g[5] * dy + g[2] * dz;
     }
     {
       T u[SQ];
@@ -802,6 +812,8 @@ GenParams<SB, SQ, T> make_params(const double* A, const double* B, const Geometr
   P.geom = geom.kind;
   P.gtab = geom.table;
   P.gstride = geom.table_stride;
+  P.gtab32 = geom.table32;
+  P.gstride32 = geom.table32_stride;
   P.kappa = geom.kappa;
   P.wdet = geom.wdet;
   P.wdet_stride = geom.wdet_stride;
@@ -824,6 +836,8 @@ void run_general(int mode, const double* A, const double* B, const Cells& cells,
   P.nz = cells.nz;
   P.mode = mode;
   if (ncells == 0) return;
+  SF_REQUIRE(sizeof(T) == 8 || mode == 2 || geom.kind != GEOM_TABLE || geom.table32, SF_ERR_STATE,
+             "internal: no FP32 copy of the geometry table");
   if (mode == 2) {
     const size_t smem = (size_t)S::EPB * DiagShape<SB, SQ>::WE * sizeof(double);
     const long long blocks = (ncells + S::EPB - 1) / S::EPB;
@@ -959,6 +973,24 @@ void launch_kappa_vjp(int dtype, int SB, int SQ, const double* A, const double* 
   else throw Error(SF_ERR_ARG, "dtype must be SF_F64 or SF_F32");
   if (!f) throw Error(SF_ERR_UNSUPPORTED, "no adjoint kernel for this SB/SQ");
   f(A, B, cells, geom, x, ybar, kbar, stream);
+}
+
+__global__ void k_table32(const double* __restrict__ src, long long total, int per,
+                          long long dst_stride, float* __restrict__ dst) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long c = i / per;
+    dst[c * dst_stride + (i - c * per)] = (float)src[i];
+  }
+}
+
+void convert_table32(const double* src, long long ncopy, int per, long long dst_stride, float* dst,
+                     cudaStream_t stream) {
+  const long long total = ncopy * per;
+  if (total == 0) return;
+  const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 16);
+  k_table32<<<(unsigned)blocks, 256, 0, stream>>>(src, total, per, dst_stride, dst);
+  SF_CUDA_CHECK(cudaGetLastError());
 }
 
 void launch_general_apply(int dtype, int SB, int SQ, const double* A, const double* B,

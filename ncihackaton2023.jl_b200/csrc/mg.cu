@@ -409,6 +409,9 @@ struct sf_mg {
   double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
   double* s = nullptr;
   double* partials = nullptr;
+  long long partials_n = 0;  // entries of partials
+  // power-iteration work vectors (largest level) and the two norms
+  double *pw_v = nullptr, *pw_w = nullptr, *pw_av = nullptr, *pw_norms = nullptr;
   double* h_s = nullptr;  // pinned copy of the scalars
   cudaStream_t cs = nullptr;  // the solver's own stream (graph capture and replay)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -645,6 +648,34 @@ void precondition(sf_mg* mg, int dt, cudaStream_t st) {
   }
 }
 
+// D^-1 in the cycle's type from the FP64 set-up copy.
+void cycle_dinv(sf_mg::Level& L, int dt, cudaStream_t st) {
+  if (dt == SF_F64)
+    SF_CUDA_CHECK(cudaMemcpyAsync(L.dinv, L.dinv64, L.n * 8, cudaMemcpyDeviceToDevice, st));
+  else
+    sf::k_convert<float, double><<<sf::grid_of(L.n), sf::kT, 0, st>>>(
+        L.dinv64, static_cast<float*>(L.dinv), L.n);
+  SF_CUDA_CHECK(cudaGetLastError());
+}
+
+// The captured iteration holds the smoother's coefficients and the kernels chosen for
+// the levels' operators; it is captured again on the next solve.
+void drop_graph(sf_mg* mg) {
+  if (mg->exec) cudaGraphExecDestroy(mg->exec);
+  if (mg->graph) cudaGraphDestroy(mg->graph);
+  mg->exec = nullptr;
+  mg->graph = nullptr;
+  mg->graph_dtype = -1;
+}
+
+// Partial-sum slots for the reductions and the operator's fused (p, A p) sums.
+void ensure_partials(sf_mg* mg) {
+  const long long need = std::max<long long>(2 * sf::kMgBlocks, sf::op_dot_partials(mg->A));
+  if (need <= mg->partials_n) return;
+  mg->partials = static_cast<double*>(mg_alloc(mg, need * sizeof(double)));
+  mg->partials_n = need;
+}
+
 // Buffers of the cycle in type dt (allocated on the first solve of that type).
 void ensure_buffers(sf_mg* mg, int dt) {
   if (mg->dtype == dt) return;
@@ -672,12 +703,7 @@ void ensure_buffers(sf_mg* mg, int dt) {
     L.d = mg_alloc(mg, L.n * es);
     L.t = mg_alloc(mg, L.n * es);
     L.r = (l == 0 && !mg->has_basis) ? nullptr : mg_alloc(mg, L.n * es);
-    if (dt == SF_F64)
-      SF_CUDA_CHECK(cudaMemcpyAsync(L.dinv, L.dinv64, L.n * 8, cudaMemcpyDeviceToDevice, mg->cs));
-    else
-      sf::k_convert<float, double><<<sf::grid_of(L.n), sf::kT, 0, mg->cs>>>(
-          L.dinv64, static_cast<float*>(L.dinv), L.n);
-    SF_CUDA_CHECK(cudaGetLastError());
+    cycle_dinv(L, dt, mg->cs);
   }
   mg->rl = mg_alloc(mg, mg->n * es);
   mg->zl = mg->has_basis ? mg_alloc(mg, mg->n * es) : nullptr;  // else level 0's current z
@@ -685,17 +711,22 @@ void ensure_buffers(sf_mg* mg, int dt) {
   mg->dtype = dt;
 }
 
-// D^-1 and lmax of every level (FP64, power iteration on D^-1 A).
+// D^-1 and lmax of every level (FP64, power iteration on D^-1 A), from the levels'
+// operators as they are now. The vectors are allocated on the first call.
 void setup_levels(sf_mg* mg, cudaStream_t st) {
-  double* norms = static_cast<double*>(mg_alloc(mg, 2 * sizeof(double)));
-  long long nmax = 0;
-  for (auto& L : mg->lv) nmax = std::max(nmax, L.n);
-  double* v = static_cast<double*>(mg_alloc(mg, nmax * 8));
-  double* w = static_cast<double*>(mg_alloc(mg, nmax * 8));
-  double* av = static_cast<double*>(mg_alloc(mg, nmax * 8));
+  if (!mg->pw_norms) {
+    long long nmax = 0;
+    for (auto& L : mg->lv) nmax = std::max(nmax, L.n);
+    mg->pw_norms = static_cast<double*>(mg_alloc(mg, 2 * sizeof(double)));
+    mg->pw_v = static_cast<double*>(mg_alloc(mg, nmax * 8));
+    mg->pw_w = static_cast<double*>(mg_alloc(mg, nmax * 8));
+    mg->pw_av = static_cast<double*>(mg_alloc(mg, nmax * 8));
+    for (auto& L : mg->lv) L.dinv64 = static_cast<double*>(mg_alloc(mg, L.n * 8));
+  }
+  double* norms = mg->pw_norms;
+  double *v = mg->pw_v, *w = mg->pw_w, *av = mg->pw_av;
   double h[2];
   for (auto& L : mg->lv) {
-    L.dinv64 = static_cast<double*>(mg_alloc(mg, L.n * 8));
     sf::op_diag(L.op, av, st);
     sf::k_invert<double><<<sf::grid_of(L.n), sf::kT, 0, st>>>(av, L.dinv64, L.n);
     sf::k_pow_next<<<sf::grid_of(L.n), sf::kT, 0, st>>>(v, nullptr, nullptr, L.n, nullptr, 1);
@@ -848,8 +879,7 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
     SF_CUDA_CHECK(cudaEventCreateWithFlags(&mg->ev_in, cudaEventDisableTiming));
     SF_CUDA_CHECK(cudaEventCreateWithFlags(&mg->ev_out, cudaEventDisableTiming));
     mg->s = static_cast<double*>(mg_alloc(mg, sf::S_NSLOTS * sizeof(double)));
-    mg->partials = static_cast<double*>(mg_alloc(
-        mg, std::max<long long>(2 * sf::kMgBlocks, sf::op_dot_partials(A)) * sizeof(double)));
+    ensure_partials(mg);
     SF_CUDA_CHECK(cudaMemsetAsync(mg->s, 0, sf::S_NSLOTS * sizeof(double), mg->cs));
     SF_CUDA_CHECK(cudaMallocHost(&mg->h_s, sf::S_NSLOTS * sizeof(double)));
     mg->x = static_cast<double*>(mg_alloc(mg, mg->n * 8));
@@ -899,10 +929,25 @@ int sf_mg_set_option(sf_mg* mg, const char* name, double value) {
     } else {
       throw Error(SF_ERR_ARG, "unknown multigrid option '" + k + "'");
     }
-    if (mg->exec) cudaGraphExecDestroy(mg->exec);
-    if (mg->graph) cudaGraphDestroy(mg->graph);
-    mg->exec = nullptr;
-    mg->graph = nullptr;
+    drop_graph(mg);
+  });
+}
+
+int sf_mg_refresh(sf_mg* mg, void* stream) {
+  if (!mg) return SF_ERR_ARG;
+  return mg_guarded(mg, [&] {
+    SF_REQUIRE(!mg->lv.empty() && mg->cs, SF_ERR_STATE, "the multigrid set-up failed");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SF_CUDA_CHECK(cudaEventRecord(mg->ev_in, st));
+    SF_CUDA_CHECK(cudaStreamWaitEvent(mg->cs, mg->ev_in, 0));
+    mg->ready = false;  // until the new diagonals and estimates are in
+    drop_graph(mg);
+    ensure_partials(mg);
+    setup_levels(mg, mg->cs);
+    if (mg->dtype >= 0)
+      for (auto& L : mg->lv) cycle_dinv(L, mg->dtype, mg->cs);
+    SF_CUDA_CHECK(cudaStreamSynchronize(mg->cs));
+    mg->ready = true;
   });
 }
 

@@ -43,6 +43,10 @@ struct Geometry {
   double G0[6] = {0};        // xx, yy, zz, xy, xz, yz
   const double* table = nullptr;  // table: [cell][6][SQ^3]
   long long table_stride = 0;     // doubles per cell (0 = one cell shared by all)
+  // FP32 copy of the table for the FP32 element kernel: [cell][6][SQ^3], rows padded to
+  // table32_stride floats (a multiple of 4; 0 = one cell shared by all)
+  const float* table32 = nullptr;
+  long long table32_stride = 0;
   const double* kappa = nullptr;  // [cell][SQ^3] or null
   const double* wdet = nullptr;   // w_q |det J| at the points, [cell][SQ^3] (the right-hand side)
   long long wdet_stride = 0;      // doubles per cell (0 = one cell shared by all)
@@ -77,6 +81,10 @@ void launch_kappa_vjp(int dtype, int SB, int SQ, const double* A, const double* 
 void launch_general_evaluate(int dtype, int SB, int SQ, const double* A, const double* B,
                              long long ncells, const int32_t* t2l, const Geometry& geom,
                              const void* x_cells, void* y_cells, cudaStream_t stream);
+
+// dst[c * dst_stride + k] = src[c * per + k] in FP32 for c < ncopy, k < per.
+void convert_table32(const double* src, long long ncopy, int per, long long dst_stride, float* dst,
+                     cudaStream_t stream);
 
 // Access to an operator handle from other translation units (sfb200.cu).
 struct OpShape {

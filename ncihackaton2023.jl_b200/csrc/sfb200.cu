@@ -36,6 +36,7 @@ struct sf_op {
   int32_t* d_t2l = nullptr;
   sf::Geometry geom;
   double* d_gtab = nullptr;
+  float* d_gtab32 = nullptr;  // FP32 copy of d_gtab (the FP32 element kernel's metric)
   double* d_wdet = nullptr;  // w |det J| at the points (right-hand side)
   double* d_kappa = nullptr;
   long long cq_cells = -1;  // -1 = unset, 0 = fill (one cell for all)
@@ -747,6 +748,7 @@ int sf_destroy(sf_op* op) {
   dfree(op->d_ids);
   dfree(op->d_t2l);
   dfree(op->d_gtab);
+  dfree(op->d_gtab32);
   dfree(op->d_wdet);
   dfree(op->d_kappa);
   dfree(op->d_diag);
@@ -982,7 +984,9 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
       }
     }
     dfree(op->d_gtab);
+    dfree(op->d_gtab32);
     op->d_gtab = nullptr;
+    op->d_gtab32 = nullptr;
     sf::Geometry g;
     g.kappa = op->d_kappa;
     if (sep) {
@@ -997,6 +1001,15 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
       g.kind = sf::GEOM_TABLE;
       g.table = op->d_gtab;
       g.table_stride = same ? 0 : 6LL * nq;
+      // the FP32 copy, each cell's rows padded to 16 bytes
+      const long long s32 = same ? 0 : (6LL * nq + 3) / 4 * 4;
+      const long long n32 = same ? 6LL * nq : ncopy * s32;
+      op->d_gtab32 = dalloc<float>((size_t)n32);
+      SF_CUDA_CHECK(cudaMemset(op->d_gtab32, 0, (size_t)n32 * sizeof(float)));
+      sf::convert_table32(op->d_gtab, ncopy, 6 * nq, same ? 0 : s32, op->d_gtab32, nullptr);
+      SF_CUDA_CHECK(cudaDeviceSynchronize());
+      g.table32 = op->d_gtab32;
+      g.table32_stride = s32;
     }
     bool wsame = true;
     for (long long c = 1; c < nc && wsame; ++c)

@@ -116,8 +116,8 @@ class Multigrid:
         if fam == "gll":  # levels[0]'s GLL basis functions at A's equispaced nodes
             basis_tab = _f64(_lagrange_values(nodes(p), np.linspace(0.0, 1.0, p + 1)))
         self._basis_tab = basis_tab
-        if A.kappa is not None:
-            self._set_coefficients(levels)
+        self._specs = levels
+        self._set_coefficients()
         ops = (C.c_void_p * len(self.levels))(*[L._h for L in self.levels])
         tab = (C.c_void_p * max(1, len(tables)))(*[t.ctypes.data for t in tables])
         for L in self.levels:  # tile shapes of the level kernels, picked once here
@@ -134,12 +134,18 @@ class Multigrid:
         self.set_option("ratio", ratio)
         self.set_option("coarse_steps", coarse_steps)
 
-    def _set_coefficients(self, levels):
+    def _set_coefficients(self):
         """A variable coefficient on the coarse levels: the operator's kappa itself on a
         level with its quadrature, else each cell's mean of it (averaged over the 8
-        children of a coarse cell on the h-levels), constant over the level's points."""
-        A = self.A
+        children of a coarse cell on the h-levels), constant over the level's points.
+        Without kappa on the operator, none on the levels either."""
+        A, levels = self.A, self._specs
         kap = A.kappa
+        if kap is None:
+            for L in self.levels:
+                if L is not A and L.kappa is not None:
+                    L.set_coefficient(None)
+            return
         if not isinstance(kap, torch.Tensor):
             kap = torch.from_numpy(np.ascontiguousarray(kap))
         kap = kap.to("cuda", torch.float64)
@@ -158,6 +164,13 @@ class Multigrid:
                 L.set_coefficient(kap)  # the same points: the operator's own kappa
             else:
                 L.set_coefficient(cell[:, None].expand(-1, nq).contiguous())
+
+    def refresh(self):
+        """Follow a new coefficient on the operator (set_coefficient): the levels get
+        its cell means and the library recomputes their diagonals and eigenvalue
+        estimates; the hierarchy itself is kept."""
+        self._set_coefficients()
+        self._err(lib.sf_mg_refresh(self._h, _stream()), "sf_mg_refresh")
 
     def close(self):
         if getattr(self, "_h", None):

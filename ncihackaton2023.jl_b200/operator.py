@@ -203,10 +203,13 @@ class LazyMatrix:
     def set_coefficient(self, kappa):
         """kappa at every quadrature point, shape (ncells, SQ^3), or None. A float64
         CUDA tensor is copied on the device; anything else is read on the host.
-        Multigrid hierarchies kept for cg(mode="mg_...") are dropped (their levels
-        hold the previous coefficient)."""
-        for mg in self.__dict__.pop("_mg", {}).values():
-            mg.close()
+        Multigrid hierarchies kept for cg(mode="mg_...") follow the new coefficient
+        (Multigrid.refresh)."""
+        self._set_kappa(kappa)
+        for mg in self.__dict__.get("_mg", {}).values():
+            mg.refresh()
+
+    def _set_kappa(self, kappa):
         if kappa is None:
             check(lib.sf_set_coefficient(self._h, None), self._h, "sf_set_coefficient")
             self.kappa = None

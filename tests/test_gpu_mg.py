@@ -128,10 +128,23 @@ def test_mg_variable_coefficient(sf):
     xs = x.cpu().numpy()
     assert np.linalg.norm(b - As @ xs) / np.linalg.norm(b) < 1e-9
     assert np.abs(xs - x_ref).max() / np.abs(x_ref).max() < 1e-7
-    # a new coefficient drops the kept hierarchy
-    assert "mg_mixed" in A._mg
-    A.set_coefficient(torch.from_numpy(kappa * 2.0).cuda())
-    assert "_mg" not in A.__dict__
+    # a new coefficient: the kept hierarchy follows it (sf_mg_refresh) and solves as a
+    # hierarchy built for that coefficient from scratch does
+    mg = A._mg["mg_mixed"]
+    kappa2 = np.exp(np.random.default_rng(9).normal(0.0, 0.5, (n ** 3, nq)))
+    A.set_coefficient(torch.from_numpy(kappa2).cuda())
+    assert A._mg["mg_mixed"] is mg
     x2, info2 = sf.cg(A, torch.from_numpy(b).cuda(), reltol=1e-10, mode="mg_mixed")
     assert info2["converged"]
-    assert np.abs(x2.cpu().numpy() - x_ref / 2.0).max() / np.abs(x_ref / 2.0).max() < 1e-7
+    x2_ref = spla.spsolve(O.assembled_sparse(om, mesh, kappa=kappa2).tocsc(), b)
+    assert np.abs(x2.cpu().numpy() - x2_ref).max() / np.abs(x2_ref).max() < 1e-7
+    fresh = sf.Multigrid(A, mode="mixed")  # (atomic sums in the applies: equal to rounding)
+    np.testing.assert_allclose(fresh.lmax(), mg.lmax(), rtol=1e-9)
+    x3, info3 = fresh.solve(torch.from_numpy(b).cuda(), reltol=1e-10)
+    assert abs(info3["iters"] - info2["iters"]) <= 1
+    fresh.close()
+    # and back to the constant coefficient
+    A.set_coefficient(None)
+    x4, info4 = sf.cg(A, torch.from_numpy(b).cuda(), reltol=1e-10, mode="mg_mixed")
+    assert info4["converged"]
+    _check_solution(om, mesh, b, x4.cpu().numpy(), 1e-7)
