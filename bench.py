@@ -877,16 +877,6 @@ def run_deformed(sf, dev, n=32, p=8, seed=5, cg_iters=1500):
                     "model_tflops": round(tf, 2), "model_tflops_frac_of_nominal_pipe":
                         round(tf / peak, 3), "nominal_pipe_tflops": round(peak, 1)}
         ys_[key] = yy.double().cpu().numpy()
-    # the FP32 apply with each cell's metric staged in shared memory by asynchronous copies
-    xx, yy = x.float(), torch.empty_like(x.float())
-    A.set_option("metric_stage", 1)
-    for _ in range(3):
-        sf.mul(yy, A, xx)
-    ms = _events_ms(lambda: sf.mul(yy, A, xx), 10)
-    A.set_option("metric_stage", 0)
-    res["f32_metric_staged"] = {"ms": round(ms, 3),
-                                "max_abs_diff_vs_f32": float(np.abs(yy.double().cpu().numpy() -
-                                                                    ys_["f32"]).max())}
     if DO_PARITY:  # the full-size applies against the C restatement (chunked geometry)
         from oracle import cref
         from oracle import sumfac_oracle as O

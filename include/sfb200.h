@@ -270,9 +270,6 @@ int sf_cgd_direction(sf_op* op, double* x, double* p, const double* r, double* s
  *   "host_groups"         : sf_mul_host with pinned buffers on the tiled kernel splits the
  *                           z-levels into this many groups of tile rows, whose copies in,
  *                           applies and copies out overlap on three streams (default 8)
- *   "metric_stage"        : 1: the FP32 element kernel (per-point metric table, SB = SQ)
- *                           copies each cell's metric into shared memory asynchronously at
- *                           the start of the element; 0 (default): loads it point by point
  *   "jacobi_table"        : 1 (default): on a whole 3D Cartesian mesh the FP64 Jacobi CG's
  *                           vector kernels read D^-1 from a table per position in a cell
  *                           (it repeats cell to cell) instead of a vector; 0: from the vector

@@ -166,22 +166,6 @@ __device__ __forceinline__ void stage_eo(const GenParams<SB, SQ, T>& P, T* sEO) 
 template <typename T>
 constexpr bool kEOParams = sizeof(T) == 4;
 
-// Staged metric (FP32, SB = SQ): words of one cell's rows of the FP32 table, a
-// multiple of 4 floats so that 16-byte asynchronous copies cover it.
-template <int SQ>
-constexpr int kStageWords = (6 * SQ * SQ * SQ + 3) / 4 * 4;
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
 // out(r, v) for r < R receives (M u)[r], M one of A, B (OP 0, 1; R = SQ, C = SB) or
 // A^T, B^T (OP 2, 3; R = SB, C = SQ). EO: through the even-odd tables in sEO
 // (about half the FMAs and matrix loads); otherwise the full matrices.
@@ -230,16 +214,11 @@ __device__ __forceinline__ void contract(const T* sMat, const T* sEO, const GenP
   }
 }
 
-// STG: the FP32 apply with a metric table stages each cell's rows of the table in
-// shared memory (after the element slots, kStageWords<SQ> floats per element) with
-// 16-byte asynchronous copies issued before the gather; the copies complete during
-// the gather and the forward passes, and the metric stage reads shared memory.
-template <int SB, int SQ, typename T, bool EO, bool STG = false>
+template <int SB, int SQ, typename T, bool EO>
 __global__ void __launch_bounds__(Shape<SB, SQ>::THREADS, Shape<SB, SQ>::MINB)
 k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   using S = Shape<SB, SQ>;
   constexpr int SM = S::SM;
-  static_assert(!STG || (sizeof(T) == 4 && SB == SQ), "staged metric: FP32, SB = SQ");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int el = threadIdx.x / S::NL;
   const int l = threadIdx.x % S::NL;
@@ -249,15 +228,6 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   T* U0 = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SL;
   T* U1 = U0 + S::SM3;
   T* U2 = U1 + S::SM3;
-  constexpr int kSlotWords = (S::EPB * S::SL + 3) / 4 * 4;  // 16-byte aligned end of the slots
-  float* sMet = reinterpret_cast<float*>(smem_raw) + kSlotWords + el * kStageWords<SQ>;
-  if constexpr (STG) {
-    if (valid) {  // the table's rows of this cell start on a 16-byte boundary
-      const float* src = P.gtab32 + cell * P.gstride32;
-      for (int k = l; k < kStageWords<SQ> / 4; k += S::NL) cp_async16(sMet + 4 * k, src + 4 * k);
-    }
-    cp_async_commit();
-  }
   __shared__ T sMat[(!EO && kStageMats<T, SB, SQ>) ? 2 * SQ * SB : 1];
   __shared__ __align__(16) T sEO[EO ? EOTables<SB, SQ>::TOTAL : 2];
   if constexpr (EO) stage_eo<SB, SQ, T>(P, sEO);
@@ -324,7 +294,6 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
     load(l2, SM, u);
     contract<0, EO, SB, SQ, T, SQ, SB>(sMat, sEO, P, u, [&](int r, T v) { l2[r * SM] = v; });
   }
-  if constexpr (STG) cp_async_wait_all();  // this thread's copies; the barrier publishes all
   __syncthreads();
 
   // ------------- z: forward, metric, backward; lines (qi,qj) -------------
@@ -364,9 +333,6 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
         const double s = P.w1[qi] * P.w1[qj] * P.w1[qk];
 #pragma unroll
         for (int c = 0; c < 6; ++c) g[c] = (T)(s * P.G0[c]);
-      } else if constexpr (STG) {
-#pragma unroll
-        for (int c = 0; c < 6; ++c) g[c] = sMet[c * SQ * SQ * SQ + q];
       } else if constexpr (sizeof(T) == 4) {
 #pragma unroll
         for (int c = 0; c < 6; ++c) g[c] = __ldg(gt32 + c * SQ * SQ * SQ + q);
@@ -882,20 +848,11 @@ void run_general(int mode, const double* A, const double* B, const Cells& cells,
     SF_CUDA_CHECK(cudaGetLastError());
     return;
   }
-  size_t smem = (size_t)S::EPB * S::SL * sizeof(T);
+  const size_t smem = (size_t)S::EPB * S::SL * sizeof(T);
   const long long blocks = (ncells + S::EPB - 1) / S::EPB;
   SF_REQUIRE(blocks < (1LL << 31), SF_ERR_ARG, "too many cells for one launch");
-  const bool eo = centro_symmetric(A, B, SB, SQ);
-  auto kern = eo ? k_general<SB, SQ, T, true> : k_general<SB, SQ, T, false>;
-  if constexpr (sizeof(T) == 4 && SB == SQ) {
-    if (eo && geom.stage && geom.kind == GEOM_TABLE && mode == 0) {
-      kern = k_general<SB, SQ, T, true, true>;
-      smem = ((size_t)S::EPB * S::SL + 3) / 4 * 4 * sizeof(T) +
-             (size_t)S::EPB * kStageWords<SQ> * sizeof(float);
-      SF_REQUIRE(geom.table32_stride % 4 == 0, SF_ERR_STATE,
-                 "internal: FP32 table rows not 16-byte aligned");
-    }
-  }
+  auto kern = centro_symmetric(A, B, SB, SQ) ? k_general<SB, SQ, T, true>
+                                             : k_general<SB, SQ, T, false>;
   SF_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<(unsigned)blocks, S::THREADS, smem, stream>>>(P);
   SF_CUDA_CHECK(cudaGetLastError());

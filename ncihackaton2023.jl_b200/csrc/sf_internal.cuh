@@ -47,9 +47,6 @@ struct Geometry {
   // table32_stride floats (a multiple of 4; 0 = one cell shared by all)
   const float* table32 = nullptr;
   long long table32_stride = 0;
-  // FP32 apply with a table (SB = SQ): copy each cell's rows of table32 into shared memory
-  // asynchronously at the start of the element instead of loading them point by point
-  bool stage = false;
   const double* kappa = nullptr;  // [cell][SQ^3] or null
   const double* wdet = nullptr;   // w_q |det J| at the points, [cell][SQ^3] (the right-hand side)
   long long wdet_stride = 0;      // doubles per cell (0 = one cell shared by all)

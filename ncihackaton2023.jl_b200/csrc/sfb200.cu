@@ -74,7 +74,6 @@ struct sf_op {
   double* d_report = nullptr;  // its device address
   double mixed_inner_reltol = 1e-1;
   int host_groups = 8;  // sf_mul_host: groups of tile rows copied in, applied and copied out
-  bool metric_stage = false;  // FP32 element kernel: stage each cell's metric in shared memory
   int last_outer = 0, last_inner = 0;
   double last_relres = 0.0;
   std::string err;
@@ -251,10 +250,8 @@ void apply_impl(sf_op* op, int dtype, const void* x, void* y, cudaStream_t st) {
              "D = 2 runs on the tiled Cartesian kernel only (axis-aligned affine cells, "
              "constant coefficient)");
   SF_CUDA_CHECK(cudaMemsetAsync(y, 0, op->n_free * es, st));
-  sf::Geometry g = op->geom;
-  g.stage = op->metric_stage;
-  sf::launch_general_apply(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, g, x, y,
-                           st);
+  sf::launch_general_apply(dtype, op->SB, op->SQ, op->A.data(), op->B.data(), op->cells, op->geom,
+                           x, y, st);
 }
 
 // diag(A) into d (n_free FP64, zeroed first): the Kronecker form on Cartesian
@@ -1006,7 +1003,7 @@ int sf_set_cell_quantities(sf_op* op, int fill, const double* wq, const double* 
       g.table_stride = same ? 0 : 6LL * nq;
       // the FP32 copy, each cell's rows padded to 16 bytes
       const long long s32 = same ? 0 : (6LL * nq + 3) / 4 * 4;
-      const long long n32 = same ? (6LL * nq + 3) / 4 * 4 : ncopy * s32;
+      const long long n32 = same ? 6LL * nq : ncopy * s32;
       op->d_gtab32 = dalloc<float>((size_t)n32);
       SF_CUDA_CHECK(cudaMemset(op->d_gtab32, 0, (size_t)n32 * sizeof(float)));
       sf::convert_table32(op->d_gtab, ncopy, 6 * nq, same ? 0 : s32, op->d_gtab32, nullptr);
@@ -1334,9 +1331,6 @@ int sf_set_option(sf_op* op, const char* name, double value) {
       SF_REQUIRE(value == -1 || value == 0 || value == 1, SF_ERR_ARG,
                  "numbered_fused must be -1 (by the numbering's locality), 0 or 1");
       op->numbered_fused = (int)value;
-    } else if (n == "metric_stage") {
-      SF_REQUIRE(value == 0 || value == 1, SF_ERR_ARG, "metric_stage must be 0 or 1");
-      op->metric_stage = value == 1;
     } else if (n == "host_groups") {
       SF_REQUIRE(value >= 1 && value <= 64 && value == (int)value, SF_ERR_ARG,
                  "host_groups must be an integer in 1..64");
