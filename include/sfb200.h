@@ -174,7 +174,7 @@ int sf_kappa_vjp(sf_op* op, int dtype, const void* x, const void* ybar, double* 
  * y = A x over the free dofs, device pointers, enqueued on `stream`
  * (a cudaStream_t, NULL = legacy default). Replaces
  * LinearAlgebra.mul!(y, A::LazyMatrix, x) (src/LazyMatrices.jl:52-61).
- * dtype SF_F64 or SF_F32 (FP32 data and accumulation, FP64 metric).
+ * dtype SF_F64 or SF_F32 (FP32: data, metric and accumulation in FP32).
  */
 int sf_apply(sf_op* op, int dtype, const void* x, void* y, void* stream);
 
