@@ -410,8 +410,7 @@ int sf_mg_refresh(sf_mg* mg, void* stream);
  * - Its scratch is one static device array sized for n_free <= SF_NOALLOC_MAX_FREE
  *   (about 10 MB). Every GPU that loads the library holds it until exit.
  *   Larger problems are rejected with SF_ERR_ARG.
- * - The first call on each device looks up the array's device address. Make
- *   that first call before any stream capture.
+ * - The first call on each device looks up the array's device address.
  * - All calls share the array: calls that overlap on the GPU race.
  */
 #define SF_NOALLOC_MAX_FREE 262144
