@@ -31,8 +31,8 @@
 // runs in FP32 and the outer CG (the caller's FP64 apply, the residual, the
 // dot products and x) stays in FP64; the reached residual is the FP64 one.
 // One outer iteration is captured once in a CUDA graph and replayed; all CG
-// scalars stay on the device and the host reads the convergence flag once per
-// few iterations. The reductions are deterministic (fixed-order sums).
+// scalars stay on the device and the host reads the convergence flag after every
+// iteration. The reductions are deterministic (fixed-order sums).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,7 +40,6 @@
 #include <cmath>
 #include <cstdlib>
 #include <string>
-#include <utility>
 #include <vector>
 
 #include "sf_internal.cuh"
@@ -51,7 +50,9 @@ namespace {
 constexpr int kT = 256;
 constexpr int kMgBlocks = 148 * 8;   // reduction grid: the partial-sum capacity
 constexpr int kMaxW = 256;           // 1D transfer table entries
-constexpr int kChunk = 4;            // iterations replayed between reads of the flag
+// Iterations replayed between reads of the convergence flag. An iteration takes milliseconds
+// and a read microseconds; with 4, a deformed Q8 32^3 solve of 18 iterations ran 20.
+constexpr int kChunk = 1;
 
 // Scalar slots of the outer FCG.
 // S_COUNTER is slot 9, where op_apply_dot's reductions keep their block counter.
@@ -61,85 +62,131 @@ enum MgSlot {
 static_assert(S_COUNTER == 9, "the reduction counter slot of op_apply_dot");
 
 // ---------------------------------------------------------------------------
-// 1D transfer pass along one axis of a structured free-point grid: out = M in
-// along the axis, with M a sparse (n_out x n_in) matrix in CSR form (start, col,
-// w), the same for every line of the grid.
+// 1D transfer pass along one axis of a structured free-point grid, cell by cell.
 // Prolongation from level l+1 to level l: the coarse grid has ncc cells of pc
 // points along the axis, the fine grid ncc cells of F points (F = r pf: r fine
-// cells of order pf per coarse cell). Fine point g (grid index 1 .. ncc F - 1)
-// lies in coarse cell c = min(g / F, ncc - 1) at local node l = g - c F, and
-//     out[g] = sum_m W[l][m] in[c pc + m]      (coarse points 1 .. ncc pc - 1).
-// The restriction is the transpose of that matrix (each fine point with the cell
-// the prolongation assigns it to, so R = P^T exactly). The host builds both
-// matrices per axis once (build_axis).
+// cells of order pf per coarse cell); W[l][m] ((F+1) x (pc+1), row-major) is the
+// coarse cell's basis function m at its fine node l. Fine point g = c F + l
+// (l < F, grid index 1 .. ncc F - 1) takes cell c's value
+//     out[g] = sum_m W[l][m] in[c pc + m]      (coarse points 1 .. ncc pc - 1),
+// and the restriction is the exact transpose: coarse point c pc + m (0 < m < pc)
+// sums W[l][m] in[c F + l] over cell c's fine points, and the vertex (c+1) pc
+// sums column pc over cell c and column 0 over cell c+1.
+// A thread takes one coarse cell of one grid line, so it loads each input of the
+// cell once; W is read from the kernel parameters (the same entry across a warp).
 // ---------------------------------------------------------------------------
-struct PassParams {
-  int n0, n1, n2;        // output grid (x fastest); n1, n2 <= 65535 (grid dimensions)
-  int axis;              // 0 x, 1 y, 2 z
-  int n_in;              // input points along the axis
-  int accumulate, subtract;  // out += ; in - in2
-  const int* start;      // CSR of the 1D matrix: n_out + 1 offsets
-  const int* col;        // input index along the axis (0-based)
-  const double* w;       // weight
+constexpr int kMaxPc = 8;     // coarse order (pc + 1 values per cell in registers)
+constexpr int kCellRows = 4;  // blocks of 32 x 4 threads
+
+template <typename T>
+struct CellPassParams {
+  T W[kMaxW];              // (F + 1) x (pc + 1), row-major
+  int F, pc, ncc;          // fine points per coarse cell, coarse order, cells along the axis
+  int n0, n1, n2;          // output grid (x fastest); the third index <= 65535
+  int n_in;                // input points along the axis
+  int axis;                // 0 x, 1 y, 2 z
+  int transpose, accumulate, subtract;  // restriction; out += ; in - in2
 };
 
-// Blocks of 32 x 8 threads: 32 consecutive outputs along x (threadIdx.x) on 8
-// grid rows (threadIdx.y), so that every warp works on one row.
-constexpr int kPassRows = 8;
-
-// Passes along y or z: each thread one output; the CSR row is the same for the
-// whole warp along y (and for the whole block along z).
-template <typename T>
-__global__ void k_pass(const __grid_constant__ PassParams Q, const T* __restrict__ in,
-                       const T* __restrict__ in2, T* __restrict__ out) {
-  const int i0 = blockIdx.x * 32 + threadIdx.x;
-  const int i1 = blockIdx.y * kPassRows + threadIdx.y;
-  const int i2 = blockIdx.z;
-  if (i0 >= Q.n0 || i1 >= Q.n1) return;
-  int idx;
-  long long base, stride;  // the axis index of the output, input base and stride
-  if (Q.axis == 1) {
-    idx = i1;
-    stride = Q.n0;
-    base = i0 + Q.n0 * (long long)Q.n_in * i2;
+// One coarse cell c of a line: ld(k) reads input point k (free index along the
+// axis), emit(k, v) writes output point k. Every output point of the line is
+// emitted by exactly one cell.
+template <typename T, typename Load, typename Emit>
+__device__ __forceinline__ void cell_pass(const CellPassParams<T>& Q, int c, const Load& ld,
+                                          const Emit& emit) {
+  const int pc = Q.pc, F = Q.F, ncc = Q.ncc;
+  if (!Q.transpose) {
+    T u[kMaxPc + 1];
+#pragma unroll
+    for (int m = 0; m <= kMaxPc; ++m) {
+      const int j = c * pc + m;  // coarse grid point (0 and ncc pc are boundary points)
+      u[m] = (m <= pc && j > 0 && j < ncc * pc) ? ld(j - 1) : T(0);
+    }
+    for (int l = 0; l < F; ++l) {
+      const int g = c * F + l;
+      if (g == 0) continue;
+      const T* w = Q.W + l * (pc + 1);
+      T acc = T(0);
+#pragma unroll
+      for (int m = 0; m <= kMaxPc; ++m)
+        if (m <= pc) acc = fma(w[m], u[m], acc);
+      emit(g - 1, acc);
+    }
   } else {
-    idx = i2;
-    stride = (long long)Q.n0 * Q.n1;
-    base = i0 + Q.n0 * (long long)i1;
+    T acc[kMaxPc + 1];
+#pragma unroll
+    for (int m = 0; m <= kMaxPc; ++m) acc[m] = T(0);
+    for (int l = 0; l < F; ++l) {
+      const int g = c * F + l;
+      const T v = g > 0 ? ld(g - 1) : T(0);
+      const T* w = Q.W + l * (pc + 1);
+#pragma unroll
+      for (int m = 1; m <= kMaxPc; ++m)
+        if (m <= pc) acc[m] = fma(w[m], v, acc[m]);
+    }
+    T vtx = T(0);  // the right vertex's part from cell c + 1 (column 0)
+    if (c + 1 < ncc)
+      for (int l = 0; l < F; ++l) vtx = fma(Q.W[l * (pc + 1)], ld((c + 1) * F + l - 1), vtx);
+#pragma unroll
+    for (int m = 1; m <= kMaxPc; ++m) {
+      const int j = c * pc + m;
+      if (m <= pc && j < ncc * pc) emit(j - 1, m == pc ? acc[m] + vtx : acc[m]);
+    }
   }
-  const int e0 = __ldg(Q.start + idx), e1 = __ldg(Q.start + idx + 1);
-  double acc = 0.0;
-  for (int e = e0; e < e1; ++e) {
-    const long long o = base + (long long)__ldg(Q.col + e) * stride;
-    const double v = Q.subtract ? (double)in[o] - (double)in2[o] : (double)in[o];
-    acc = fma(__ldg(Q.w + e), v, acc);
-  }
-  const long long o = i0 + Q.n0 * (i1 + Q.n1 * (long long)i2);
-  if (Q.accumulate) out[o] = (T)((double)out[o] + acc);
-  else out[o] = (T)acc;
 }
 
-// The pass along x: each warp takes one grid row, stages its inputs (in - in2) in
-// shared memory with coalesced loads, and gathers its outputs from there.
+// Passes along y (axis 1) or z (axis 2): thread (x, cell, third index); the loads
+// and stores of a warp are consecutive along x.
 template <typename T>
-__global__ void k_pass_x(const __grid_constant__ PassParams Q, const T* __restrict__ in,
-                         const T* __restrict__ in2, T* __restrict__ out) {
-  extern __shared__ double srow[];
-  const int i1 = blockIdx.y * kPassRows + threadIdx.y, i2 = blockIdx.z;
-  if (i1 >= Q.n1) return;  // the whole warp
-  double* row = srow + threadIdx.y * Q.n_in;
-  const long long ibase = (long long)Q.n_in * (i1 + Q.n1 * (long long)i2);
-  for (int k = threadIdx.x; k < Q.n_in; k += 32)
-    row[k] = Q.subtract ? (double)in[ibase + k] - (double)in2[ibase + k] : (double)in[ibase + k];
-  __syncwarp();
-  const long long obase = (long long)Q.n0 * (i1 + Q.n1 * (long long)i2);
-  for (int i0 = threadIdx.x; i0 < Q.n0; i0 += 32) {
-    const int e0 = __ldg(Q.start + i0), e1 = __ldg(Q.start + i0 + 1);
-    double acc = 0.0;
-    for (int e = e0; e < e1; ++e) acc = fma(__ldg(Q.w + e), row[__ldg(Q.col + e)], acc);
-    if (Q.accumulate) out[obase + i0] = (T)((double)out[obase + i0] + acc);
-    else out[obase + i0] = (T)acc;
+__global__ void k_cellpass(const __grid_constant__ CellPassParams<T> Q, const T* __restrict__ in,
+                           const T* __restrict__ in2, T* __restrict__ out) {
+  const int i0 = blockIdx.x * 32 + threadIdx.x;
+  const int c = blockIdx.y * kCellRows + threadIdx.y;
+  const int io = blockIdx.z;  // z for a pass along y, y for a pass along z
+  if (i0 >= Q.n0 || c >= Q.ncc) return;
+  long long ib, ob, stride;
+  if (Q.axis == 1) {
+    stride = Q.n0;
+    ib = i0 + (long long)Q.n0 * Q.n_in * io;
+    ob = i0 + (long long)Q.n0 * Q.n1 * io;
+  } else {
+    stride = (long long)Q.n0 * Q.n1;
+    ib = ob = i0 + (long long)Q.n0 * io;
   }
+  cell_pass<T>(
+      Q, c,
+      [&](int k) {
+        const long long o = ib + k * stride;
+        return Q.subtract ? in[o] - in2[o] : in[o];
+      },
+      [&](int k, T v) {
+        const long long o = ob + k * stride;
+        out[o] = Q.accumulate ? out[o] + v : v;
+      });
+}
+
+// The pass along x: a warp per grid row stages the row's inputs (in - in2) in
+// shared memory with coalesced loads, assembles the output row there cell by
+// cell, and stores it coalesced.
+template <typename T>
+__global__ void k_cellpass_x(const __grid_constant__ CellPassParams<T> Q,
+                             const T* __restrict__ in, const T* __restrict__ in2,
+                             T* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char cp_smem[];
+  T* srow = reinterpret_cast<T*>(cp_smem) + threadIdx.y * (Q.n_in + Q.n0);
+  T* sout = srow + Q.n_in;
+  const int i1 = blockIdx.y * kCellRows + threadIdx.y, i2 = blockIdx.z;
+  if (i1 >= Q.n1) return;  // the whole warp
+  const long long ib = (long long)Q.n_in * (i1 + (long long)Q.n1 * i2);
+  const long long ob = (long long)Q.n0 * (i1 + (long long)Q.n1 * i2);
+  for (int k = threadIdx.x; k < Q.n_in; k += 32)
+    srow[k] = Q.subtract ? in[ib + k] - in2[ib + k] : in[ib + k];
+  __syncwarp();
+  for (int c = threadIdx.x; c < Q.ncc; c += 32)
+    cell_pass<T>(Q, c, [&](int k) { return srow[k]; }, [&](int k, T v) { sout[k] = v; });
+  __syncwarp();
+  for (int k = threadIdx.x; k < Q.n0; k += 32)
+    out[ob + k] = Q.accumulate ? out[ob + k] + sout[k] : sout[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -382,10 +429,6 @@ struct sf_mg {
   struct Transfer {
     int r = 1, F = 0, pc = 0;
     std::vector<double> W;  // (F + 1) x (pc + 1)
-    // device CSR of the 1D prolongation (mode 0) and restriction (mode 1) per axis
-    const int* start[2][3] = {};
-    const int* col[2][3] = {};
-    const double* w[2][3] = {};
   };
   sf_op* A = nullptr;  // the caller's operator (the outer FP64 CG)
   long long n = 0;
@@ -467,80 +510,43 @@ int mg_guarded(sf_mg* mg, F&& f) {
 
 size_t esize(int dtype) { return dtype == SF_F64 ? 8 : 4; }
 
-// One 1D pass. in/out grids: out dims (n0, n1, n2); the input has n_in points
-// along the axis.
+// One 1D pass of transfer t along `axis` (ncc coarse cells along it). out dims
+// (n0, n1, n2); the input has n_in points along the axis.
 template <typename T>
 void pass(const sf_mg::Transfer& t, int axis, bool transpose, long long n0, long long n1,
-          long long n2, int n_in, const T* in, const T* in2, T* out, bool acc, cudaStream_t st) {
-  sf::PassParams Q{};
+          long long n2, int n_in, int ncc, const T* in, const T* in2, T* out, bool acc,
+          cudaStream_t st) {
+  if (n0 <= 0 || n1 <= 0 || n2 <= 0) return;
+  sf::CellPassParams<T> Q{};
+  for (size_t i = 0; i < t.W.size(); ++i) Q.W[i] = (T)t.W[i];
+  Q.F = t.F;
+  Q.pc = t.pc;
+  Q.ncc = ncc;
   Q.n0 = (int)n0;
   Q.n1 = (int)n1;
   Q.n2 = (int)n2;
   Q.axis = axis;
   Q.n_in = n_in;
+  Q.transpose = transpose ? 1 : 0;
   Q.accumulate = acc ? 1 : 0;
   Q.subtract = in2 ? 1 : 0;
-  const int mode = transpose ? 1 : 0;
-  Q.start = t.start[mode][axis];
-  Q.col = t.col[mode][axis];
-  Q.w = t.w[mode][axis];
-  if (n0 <= 0 || n1 <= 0 || n2 <= 0) return;
-  SF_REQUIRE(n2 <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
-  const dim3 block(32, sf::kPassRows);
-  const unsigned gy = (unsigned)((n1 + sf::kPassRows - 1) / sf::kPassRows);
-  if (axis == 0 && n_in <= 768) {  // rows staged in shared memory (8 x n_in doubles)
-    sf::k_pass_x<T><<<dim3(1, gy, (unsigned)n2), block,
-                      (size_t)sf::kPassRows * n_in * sizeof(double), st>>>(Q, in, in2, out);
+  const dim3 block(32, sf::kCellRows);
+  if (axis == 0) {  // rows staged in shared memory: kCellRows x (n_in + n0) values
+    SF_REQUIRE(n_in <= 767 && n0 <= 767 && n2 <= 65535, SF_ERR_UNSUPPORTED,
+               "multigrid transfer: at most 767 free points per grid row");
+    const size_t smem = (size_t)sf::kCellRows * (n_in + n0) * sizeof(T);
+    sf::k_cellpass_x<T><<<dim3(1, (unsigned)((n1 + sf::kCellRows - 1) / sf::kCellRows),
+                               (unsigned)n2),
+                          block, smem, st>>>(Q, in, in2, out);
   } else {
-    SF_REQUIRE(axis != 0, SF_ERR_UNSUPPORTED, "multigrid transfer: grid rows too long");
-    sf::k_pass<T><<<dim3((unsigned)((n0 + 31) / 32), gy, (unsigned)n2), block, 0, st>>>(
-        Q, in, in2, out);
+    const long long third = axis == 1 ? n2 : n1;
+    SF_REQUIRE(third <= 65535, SF_ERR_UNSUPPORTED, "multigrid transfer: grid too large");
+    sf::k_cellpass<T><<<dim3((unsigned)((n0 + 31) / 32),
+                             (unsigned)((ncc + sf::kCellRows - 1) / sf::kCellRows),
+                             (unsigned)third),
+                        block, 0, st>>>(Q, in, in2, out);
   }
   SF_CUDA_CHECK(cudaGetLastError());
-}
-
-// The 1D prolongation and restriction matrices of transfer t along every axis
-// (ncc coarse cells along each), built on the host and copied to the device.
-void build_tables(sf_mg* mg, sf_mg::Transfer& t, const int ncc[3]) {
-  for (int axis = 0; axis < 3; ++axis) {
-    const int n = ncc[axis], nf = n * t.F - 1, nc = n * t.pc - 1;
-    std::vector<std::vector<std::pair<int, double>>> P(std::max(nf, 0)), R(std::max(nc, 0));
-    for (int g = 1; g < n * t.F; ++g) {
-      const int c = std::min(g / t.F, n - 1);
-      const int l = g - c * t.F;
-      for (int m = 0; m <= t.pc; ++m) {
-        const int j = c * t.pc + m;
-        const double w = t.W[l * (t.pc + 1) + m];
-        if (j > 0 && j < n * t.pc && w != 0.0) {
-          P[g - 1].push_back({j - 1, w});
-          R[j - 1].push_back({g - 1, w});
-        }
-      }
-    }
-    for (int mode = 0; mode < 2; ++mode) {
-      const auto& M = mode == 0 ? P : R;
-      std::vector<int> start(1, 0), col;
-      std::vector<double> w;
-      for (const auto& row : M) {
-        for (const auto& e : row) {
-          col.push_back(e.first);
-          w.push_back(e.second);
-        }
-        start.push_back((int)col.size());
-      }
-      int* ds = static_cast<int*>(mg_alloc(mg, start.size() * sizeof(int)));
-      int* dc = static_cast<int*>(mg_alloc(mg, std::max<size_t>(col.size(), 1) * sizeof(int)));
-      double* dw = static_cast<double*>(mg_alloc(mg, std::max<size_t>(w.size(), 1) * sizeof(double)));
-      SF_CUDA_CHECK(cudaMemcpy(ds, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
-      if (!col.empty()) {
-        SF_CUDA_CHECK(cudaMemcpy(dc, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
-        SF_CUDA_CHECK(cudaMemcpy(dw, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
-      }
-      t.start[mode][axis] = ds;
-      t.col[mode][axis] = dc;
-      t.w[mode][axis] = dw;
-    }
-  }
 }
 
 // out (fine grid, fx x fy x fz free points) (+)= P in (coarse grid cx x cy x cz);
@@ -554,9 +560,9 @@ void prolong(sf_mg* mg, const sf_mg::Transfer& t, const int ncc[3], const T* in,
                           (long long)ncc[2] * t.F - 1};
   T* a = static_cast<T*>(mg->tmp1);
   T* b = static_cast<T*>(mg->tmp2);
-  pass<T>(t, 2, false, c[0], c[1], f[2], (int)c[2], in, nullptr, a, false, st);
-  pass<T>(t, 1, false, c[0], f[1], f[2], (int)c[1], a, nullptr, b, false, st);
-  pass<T>(t, 0, false, f[0], f[1], f[2], (int)c[0], b, nullptr, out, acc, st);
+  pass<T>(t, 2, false, c[0], c[1], f[2], (int)c[2], ncc[2], in, nullptr, a, false, st);
+  pass<T>(t, 1, false, c[0], f[1], f[2], (int)c[1], ncc[1], a, nullptr, b, false, st);
+  pass<T>(t, 0, false, f[0], f[1], f[2], (int)c[0], ncc[0], b, nullptr, out, acc, st);
 }
 
 // out (coarse) = P^T (in - in2) (fine); in2 may be null.
@@ -569,9 +575,9 @@ void restrict_(sf_mg* mg, const sf_mg::Transfer& t, const int ncc[3], const T* i
                           (long long)ncc[2] * t.F - 1};
   T* a = static_cast<T*>(mg->tmp1);
   T* b = static_cast<T*>(mg->tmp2);
-  pass<T>(t, 0, true, c[0], f[1], f[2], (int)f[0], in, in2, a, false, st);
-  pass<T>(t, 1, true, c[0], c[1], f[2], (int)f[1], a, nullptr, b, false, st);
-  pass<T>(t, 2, true, c[0], c[1], c[2], (int)f[2], b, nullptr, out, false, st);
+  pass<T>(t, 0, true, c[0], f[1], f[2], (int)f[0], ncc[0], in, in2, a, false, st);
+  pass<T>(t, 1, true, c[0], c[1], f[2], (int)f[1], ncc[1], a, nullptr, b, false, st);
+  pass<T>(t, 2, true, c[0], c[1], c[2], (int)f[2], ncc[2], b, nullptr, out, false, st);
 }
 
 template <typename T>
@@ -850,7 +856,8 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
       t.r = r;
       t.F = r * F.p;
       t.pc = C.p;
-      SF_REQUIRE((t.F + 1) * (t.pc + 1) <= sf::kMaxW, SF_ERR_ARG, "transfer table too large");
+      SF_REQUIRE((t.F + 1) * (t.pc + 1) <= sf::kMaxW && t.pc <= sf::kMaxPc, SF_ERR_ARG,
+                 "transfer table too large");
       SF_REQUIRE(F.nx * F.p <= 768 && F.nz * F.p <= 65535, SF_ERR_UNSUPPORTED,
                  "multigrid transfer: at most 767 free points per grid row");
       t.W.assign(transfer[l], transfer[l] + (t.F + 1) * (t.pc + 1));
@@ -861,19 +868,11 @@ int sf_mg_create(sf_mg** out, sf_op* A, int nlevels, sf_op* const* levels,
       mg->basis.r = 1;
       mg->basis.F = L0.p;
       mg->basis.pc = L0.p;
-      SF_REQUIRE((L0.p + 1) * (L0.p + 1) <= sf::kMaxW, SF_ERR_ARG, "basis table too large");
+      SF_REQUIRE((L0.p + 1) * (L0.p + 1) <= sf::kMaxW && L0.p <= sf::kMaxPc, SF_ERR_ARG,
+                 "basis table too large");
       SF_REQUIRE(L0.nx * L0.p <= 768, SF_ERR_UNSUPPORTED,
                  "multigrid transfer: at most 767 free points per grid row");
       mg->basis.W.assign(basis_change, basis_change + (L0.p + 1) * (L0.p + 1));
-    }
-    for (int l = 0; l + 1 < nlevels; ++l) {
-      const auto& C = mg->lv[l + 1];
-      const int ncc[3] = {C.nx, C.ny, C.nz};
-      build_tables(mg, mg->tr[l], ncc);
-    }
-    if (mg->has_basis) {
-      const int ncc[3] = {L0.nx, L0.ny, L0.nz};
-      build_tables(mg, mg->basis, ncc);
     }
     SF_CUDA_CHECK(cudaStreamCreateWithFlags(&mg->cs, cudaStreamNonBlocking));
     SF_CUDA_CHECK(cudaEventCreateWithFlags(&mg->ev_in, cudaEventDisableTiming));
