@@ -230,6 +230,17 @@ k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   const int l = threadIdx.x % S::NL;
   const long long cell = (long long)blockIdx.x * S::EPB + el;
   const bool valid = cell < P.ncells;
+  // One thread per element asks for the element's row of the metric table in L2: it
+  // arrives while the gather and the forward passes run, and the metric stage's loads
+  // then hit L2. The row starts on a 16-byte boundary (6 SQ^3 doubles, or the padded
+  // FP32 row); the size is rounded down to 16 bytes, so it stays inside the row.
+  if (P.geom == GEOM_TABLE && valid && l == 0) {
+    const void* row = sizeof(T) == 4 ? static_cast<const void*>(P.gtab32 + cell * P.gstride32)
+                                     : static_cast<const void*>(P.gtab + cell * P.gstride);
+    constexpr unsigned kRowBytes = (unsigned)(6 * SQ * SQ * SQ * sizeof(T)) & ~15u;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(kRowBytes)
+                 : "memory");
+  }
 
   T* U0 = reinterpret_cast<T*>(smem_raw) + (size_t)el * S::SL;
   T* U1 = U0 + S::SM3;
