@@ -1004,10 +1004,13 @@ template <> struct Cands<4, double> { static constexpr Candidate c[] = {SF_TILE(
                                                                       SF_TILE(4, double, 4, 4, 3, 320, 2),
                                                                       SF_TILE(4, double, 4, 4, 1, 128, 6),
                                                                       SF_TILE(4, double, 8, 4, 2, 256, 2)}; };
-template <> struct Cands<5, double> { static constexpr Candidate c[] = {SF_TILE(5, double, 2, 2, 2, 256, 2),
+// Q5 2x2x3 at three CTAs per SM and Q6 2x2x2 at two were the fastest FP64 shapes on 20^3 and
+// 36^3 (Q5: 0.0168 / 0.0664 ms) and on 16^3 (Q6: 0.0168 ms; 2x3x2 on 30^3, 0.0739 ms).
+template <> struct Cands<5, double> { static constexpr Candidate c[] = {SF_TILE(5, double, 2, 2, 3, 256, 3),
+                                                                      SF_TILE(5, double, 2, 2, 2, 256, 2),
                                                                       SF_TILE(5, double, 2, 3, 3, 256, 2),
                                                                       SF_TILE(5, double, 2, 4, 2, 256, 2)}; };
-template <> struct Cands<6, double> { static constexpr Candidate c[] = {SF_TILE(6, double, 2, 2, 2, 256, 1),
+template <> struct Cands<6, double> { static constexpr Candidate c[] = {SF_TILE(6, double, 2, 2, 2, 256, 2),
                                                                       SF_TILE(6, double, 2, 3, 2, 256, 2)}; };
 template <> struct Cands<7, double> { static constexpr Candidate c[] = {SF_TILE(7, double, 2, 2, 1, 256, 1),
                                                                       SF_TILE(7, double, 2, 2, 2, 256, 1)}; };
