@@ -69,7 +69,8 @@ def test_all_orders(sf, p):
         assert relerr(y, y_ref) < TOL64, (p, deg)
 
 
-@pytest.mark.parametrize("p,deg", [(2, 4), (3, 6), (4, 8), (4, 6)])
+@pytest.mark.parametrize("p,deg", [(2, 4), (3, 6), (4, 8), (4, 6), (5, 10), (6, 12), (7, 14),
+                                   (8, 16)])
 def test_every_tile_candidate(sf, p, deg):
     """Every tile shape the autotuner may pick gives the oracle's result, on a
     mesh that is not a multiple of any tile (partial tiles at the far faces)."""
