@@ -363,8 +363,8 @@ const char* sf_batch_group_kernel(const sf_batch* b, int dtype, int group);
  * sf_mg_cg: x (device, FP64, initial guess on entry) solves A x = b to
  * ||b - A x|| <= reltol ||b||. mode SF_MG_MIXED runs the V-cycle in FP32 (outer
  * CG, residual and dots in FP64), SF_MG_F64 all in FP64; one handle solves in
- * one mode. Options (sf_mg_set_option): "degree" (Chebyshev smoothing steps, 3),
- * "ratio" (smoothing range lmax/ratio..1.1 lmax, 30), "coarse_steps" (10),
+ * one mode. Options (sf_mg_set_option): "degree" (Chebyshev smoothing steps, 4),
+ * "ratio" (smoothing range lmax/ratio..1.1 lmax, 20), "coarse_steps" (10),
  * "coarse_ratio" (100). sf_mg_get_info: "levels", "lmax<l>", "n<l>", "graph".
  *
  * sf_mg_refresh: after the operators' coefficients changed (sf_set_coefficient

@@ -69,8 +69,8 @@ class Multigrid:
     coarse_steps: Chebyshev steps on the coarsest level.
     """
 
-    def __init__(self, A: LazyMatrix, mode: str = "mixed", basis: str = "auto", degree: int = 3,
-                 ratio: float = 30.0, h_levels: bool = True, coarse_steps: int = 10,
+    def __init__(self, A: LazyMatrix, mode: str = "mixed", basis: str = "auto", degree: int = 4,
+                 ratio: float = 20.0, h_levels: bool = True, coarse_steps: int = 10,
                  min_cells: int = 8):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
