@@ -79,7 +79,6 @@ struct Shape {
   static constexpr int SM3 = SM * SM * SM;
   static constexpr int SL = 3 * SM3;  // words per element of k_general (three padded slots)
   static constexpr int MINB = 2;      // CTAs per SM asked of the register allocator
-  static constexpr int MINB_APPLY = 4;  // the same for k_general
 };
 
 // Global free index of tensor position `pos` of cell `c` on the structured mesh, or -1.
@@ -219,9 +218,13 @@ __device__ __forceinline__ void contract(const T* sMat, const T* sEO, const GenP
 // threads): the kernel waits on its metric and gather loads, and a fourth CTA hides more of
 // that than the registers cost. Measured against three CTAs (deformed Q8 32^3; Q4 64^3 table
 // gather): FP32 0.444 -> 0.378 ms and 0.565 -> 0.433 ms, FP64 0.723 -> 0.712 ms and
-// 0.948 -> 0.912 ms (no spills at Q8 FP64, 24 bytes at Q8 FP32).
+// 0.948 -> 0.912 ms (no spills at Q8 FP64, 24 bytes at Q8 FP32). FP32 elements of 9 or more
+// points per axis ask for five (deformed Q8 FP32 0.362 -> 0.341 ms with 80 bytes of spills; at
+// Q4 five were 1 % slower).
+template <typename T, int SM>
+constexpr int kMinbApply = sizeof(T) == 4 && SM >= 9 ? 5 : 4;
 template <int SB, int SQ, typename T, bool EO>
-__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS, Shape<SB, SQ>::MINB_APPLY)
+__global__ void __launch_bounds__(Shape<SB, SQ>::THREADS, kMinbApply<T, Shape<SB, SQ>::SM>)
 k_general(const __grid_constant__ GenParams<SB, SQ, T> P) {
   using S = Shape<SB, SQ>;
   constexpr int SM = S::SM;
